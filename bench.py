@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""Benchmark of the stochastic-KPM hot path (KPM moment recurrence).
+
+Workload (one "step"): the Jackson-KPM moments mu_0..mu_{M-1} of R random-phase
+vectors on the honeycomb lattice of 2048 x 1024 cells x 2 = 4,194,304 sites
+(t = -2.7 eV, Anderson disorder in [-1, 1] eV), R = 64 vectors in one block,
+M = 4096 moments, spectral window (-9.2, 9.2) eV.  B200 arm: the mixed form
+(complex64 vectors and SpMM, FP64 moment accumulation) with the product
+identity for the moments; the plain FP64 path is measured beside it.  Work is
+counted as N * M * R orbital*moment*vec per step.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One process per GPU (torchrun for N > 1): every rank owns R independent
+vectors (its statistics block; replicated H), no collective in the timed
+region (weak scaling); the step time is the max over ranks.
+`--impl reference` times KuboMSD's own compiled CPU engine (cpp/native.cpp,
+built into oracle/_ref/) on this host's cores for the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "orbital·moment·vec/s mixed vs FP64 @MSD relerr≤1e-4; HBM GB/s; p50/p99 latency"
+UNIT = "orbital·moment·vec/s"
+BOUNDS = (-9.2, 9.2)
+FALLBACK_HBM_GBS = 6650.0
+# dram bytes per launch of the dominant kernel from the ncu capture summarised in
+# profiles/cheb_step_doubling_f32_honeycomb.md (None until captured).
+NCU_TRAFFIC_PER_LAUNCH = None
+
+
+def parse():
+    p = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--lx", type=int, default=2048)
+    p.add_argument("--ly", type=int, default=1024)
+    p.add_argument("--vectors", type=int, default=64)
+    p.add_argument("--moments", type=int, default=4096)
+    p.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    p.add_argument("--method", choices=["doubling", "direct"], default="doubling")
+    p.add_argument("--no-compare", action="store_true", help="skip the FP64 / direct comparison lines")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def config(args, n):
+    return {"workload": f"KPM moments, honeycomb {args.lx}x{args.ly}x2 = {n:,} sites, R={args.vectors}, "
+                        f"M={args.moments}", "sites": n, "vectors_per_gpu": args.vectors, "moments": args.moments,
+            "spectral_bounds_eV": list(BOUNDS), "disorder_eV": [-1., 1.], "hopping_eV": -2.7,
+            "precision": args.precision, "moment_method": args.method,
+            "l2_policy": "inputs larger than L2 (vector blocks of 2.1-4.3 GB per buffer)",
+            "parallelism": f"dp{args.gpus} (statistics blocks per GPU, replicated H)"}
+
+
+def peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        d = json.loads(path.read_text())
+        return float(d.get("hbm_gbs", FALLBACK_HBM_GBS)), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(suffix=".csv")[1])
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(H, n, threads, R=8, M=4):
+    """KuboMSD's compiled CPU engine (oracle/_ref) on a bounded sample of the workload."""
+    from oracle import ref_native
+    import scipy.sparse as sp
+    mod = ref_native.load()
+    kind = "reference"
+    B = np.exp(2j * np.pi * np.random.default_rng(9).random((n, R)))
+    c, a = (BOUNDS[0] + BOUNDS[1]) / 2, (BOUNDS[1] - BOUNDS[0]) / 2
+    if mod is not None:
+        eng = ref_native.RefEngine(H, sp.identity(n, format="csr"), threads=threads)
+        run = lambda: eng.core.moments(B, M, c, a)  # noqa: E731
+    else:  # the oracle restatement when the reference binary is absent
+        from oracle import kpm_oracle as O
+        eng = O.engine_from_model(H, sp.identity(n, format="csr"))
+        run = lambda: eng.moments(B, M, c, a)  # noqa: E731
+        kind, threads = "port", 1
+    t0 = time.perf_counter()
+    run()
+    dt = time.perf_counter() - t0
+    return {"value": n * M * R / dt, "unit": UNIT, "cores": threads, "kind": kind, "seconds": dt,
+            "sample": f"one moments call, R={R} vectors, M={M} moments on the full {n:,}-site lattice "
+                      f"({threads} OpenMP threads)"}
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return
+    from kubomsd_b200 import lattices
+    m = lattices.honeycomb(args.lx, args.ly, with_velocity=False)
+    threads = len(os.sched_getaffinity(0))
+    R, M = 8, 4
+    for _ in range(args.warmup):
+        cpu_baseline(m.H, m.n, threads, R, M)
+    times = [cpu_baseline(m.H, m.n, threads, R, M) for _ in range(args.steps)]
+    sec = sum(t["seconds"] for t in times) / len(times)
+    value = m.n * M * R / sec
+    cb = dict(times[0])
+    cb["value"] = value
+    cb.pop("seconds", None)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded lattice and phases)",
+            "config": {**config(args, m.n), "reference_sample": cb["sample"]}, "cpu_baseline": cb,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+    from types import SimpleNamespace
+    from kubomsd_b200 import _abi, kpm, lattices
+    from kubomsd_b200.native import B200Metric, B200Operators
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    lib = _abi.require_library()
+    m = lattices.honeycomb(args.lx, args.ly, with_velocity=False)
+    n, R, M = m.n, args.vectors, args.moments
+    # this rank's statistics block: sample ids rank*R .. rank*R+R-1
+    host = torch.empty((n, R), dtype=torch.complex128, pin_memory=True)
+    host.numpy()[:] = kpm.random_phases(n, 20261019, range(rank * R, rank * R + R))
+    B = host.to("cuda", non_blocking=False)
+    c, a = (BOUNDS[0] + BOUNDS[1]) / 2, (BOUNDS[1] - BOUNDS[0]) / 2
+
+    def engine(precision, method):
+        cfg = SimpleNamespace(metric_rtol=1e-10, metric_atol=0., metric_maxiter=1000,
+                              metric_residual_policy="fixed", metric_check_interval=32, metric_gap_ratio=.1,
+                              metric_solver="pcg", precision=precision, moment_doubling=method == "doubling")
+        metric = B200Metric(m.S, np.ones(n), [], cfg)
+        ops = SimpleNamespace(host_H=m.H, metric=SimpleNamespace(native=metric), velocity={}, position={},
+                              composite={})
+        return B200Operators(ops, cfg)
+
+    eng = engine(args.precision, args.method)
+    for _ in range(args.warmup):
+        eng.moments(B, M, c, a)
+    stream = torch.cuda.current_stream()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(torch.cuda.current_device()) if rank == 0 else None
+    l0 = lib.kmsd_kernel_launches()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        mu = eng.moments(B, M, c, a)
+    end.record(stream)
+    torch.cuda.synchronize()
+    launches = lib.kmsd_kernel_launches() - l0
+    clk = clocks.stop() if clocks else None
+    ms = start.elapsed_time(end)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_step = ms / args.steps
+    value = world * n * M * R / (ms_step / 1e3)
+    mu_host = mu.cpu().numpy()
+    assert np.allclose(mu_host[0], n, rtol=1e-6), "mu_0 must equal the vector norm N"
+
+    # dominant kernel: one fused Chebyshev step per operator application
+    C = 2 if args.precision == "mixed" else 1
+    unit_bytes = 16
+    row_bytes_vec = (R // C) * unit_bytes if R % C == 0 else ((R + 1) // 2) * unit_bytes
+    nnz_row = m.H.nnz / n
+    mat_bytes = 4 + nnz_row * (4 + (4 if args.precision == "mixed" else 8))
+    passes = 3 if args.method == "doubling" else 4
+    launches_per_step = (M + 1) // 2 if args.method == "doubling" else M - 1
+    bytes_per_launch = n * (passes * row_bytes_vec + mat_bytes)
+    avg_launch_s = (ms_step / 1e3) / launches_per_step
+    achieved = bytes_per_launch / avg_launch_s / 1e9
+    peak, peak_src = peaks()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": NCU_TRAFFIC_PER_LAUNCH, "peak_source": peak_src, "kernel": "cheb_step_kernel",
+            "algorithmic_bytes_per_launch": bytes_per_launch, "launches_per_step": launches_per_step,
+            "bytes_per_omv": bytes_per_launch / (n * R * (2 if args.method == "doubling" else 1)),
+            "timing": "step time / launches per step (includes the 3 small set-up kernels of each step)"}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64 vectors / f64 accumulation" if args.precision == "mixed" else "c128",
+            "data": "synthetic (seeded honeycomb lattice, NumPy PCG64 random phases)",
+            "config": config(args, n), "roofline": roof, "gpu_launches": int(launches), "clocks": clk}
+
+    # end to end through the reference-facing plugin call with host buffers
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    hostB = host.numpy()
+    t0 = time.perf_counter()
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for _ in range(args.steps):
+        out = eng.moments(hostB, M, c, a)   # numpy in -> numpy out (H2D + D2H inside)
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    e_ms = e_start.elapsed_time(e_end)
+    wall = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_ms = float(t.item())
+    assert isinstance(out, np.ndarray) and out.shape == (M, R)
+    line["e2e"] = {"value": world * n * M * R / (e_ms / args.steps / 1e3), "unit": UNIT,
+                   "h2d_bytes_per_step": int(n * R * 16), "d2h_bytes_per_step": int(M * R * 8),
+                   "ms_per_step": e_ms / args.steps, "host_wall_ms_per_step": wall / args.steps * 1e3,
+                   "call": "B200Operators.moments(numpy complex128 (N,R) from pinned memory) -> numpy (M,R)"}
+
+    if world == 1 and not args.no_compare:
+        compare = {}
+        for prec, meth in (("fp64", "direct"), ("fp64", "doubling"), ("mixed", "direct")):
+            if (prec, meth) == (args.precision, args.method):
+                continue
+            e2 = engine(prec, meth)
+            e2.moments(B, M, c, a)
+            torch.cuda.synchronize()
+            s2, t2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s2.record(stream)
+            mu2 = e2.moments(B, M, c, a)
+            t2.record(stream)
+            torch.cuda.synchronize()
+            v2 = n * M * R / (s2.elapsed_time(t2) / 1e3)
+            err = float(np.max(np.abs(mu_host - mu2.cpu().numpy())) / np.max(np.abs(mu2.cpu().numpy())))
+            compare[f"{prec}_{meth}"] = {"value": v2, "ms_per_step": s2.elapsed_time(t2),
+                                         "moments_relerr_vs_headline": err}
+            del e2
+            torch.cuda.empty_cache()
+        line["compare"] = compare
+        if "fp64_direct" in compare:
+            line["speedup_vs_fp64_direct"] = value / compare["fp64_direct"]["value"]
+        line["msd_check"] = msd_check()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(m.H, n, len(os.sched_getaffinity(0)))
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def msd_check():
+    """Mixed vs FP64 stepwise MSD on the 64x64 square lattice (R=8, M=512,
+    0-10 fs): the tolerance the mixed form is held to (untimed)."""
+    import torch
+    from kubomsd_b200 import kpm, lattices, stochastic
+    from kubomsd_b200.config import RunConfig
+    from kubomsd_b200.operators import build_operators
+    m = lattices.square_lattice(64)
+    B = kpm.random_phases(m.n, 20261019, range(8))
+    out = {}
+    for prec in ("fp64", "mixed"):
+        cfg = RunConfig(energy_eV=np.linspace(-11, 11, 201), time_fs=np.arange(11.), spectral_bounds=(-11.2, 11.2),
+                        n_moments=512, axes=("x",), include_vac=False, stochastic_method="stepwise", precision=prec)
+        ops = build_operators(m, cfg)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dos, nums, _ = stochastic.stepwise_samples(ops, cfg, B)
+        out[prec] = (dos, nums["msd_A2/commutator"], time.perf_counter() - t0)
+    d64, m64, t64 = out["fp64"]
+    d32, m32, t32 = out["mixed"]
+    return {"case": "64x64 square, R=8, M=512, 0-10 fs dt=1 fs, 201 energies",
+            "msd_relerr": float(np.max(np.abs(m32 - m64)) / np.max(np.abs(m64))),
+            "dos_relerr": float(np.max(np.abs(d32 - d64)) / np.max(np.abs(d64))),
+            "fp64_seconds": t64, "mixed_seconds": t32}
+
+
+if __name__ == "__main__":
+    main()

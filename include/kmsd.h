@@ -1,0 +1,248 @@
+/*
+ * kmsd.h — C ABI of the B200 stochastic-KPM transport engine (libkmsd_b200.so).
+ *
+ * The library replaces the compiled CPU engine of KuboMSD (`kubo_msd._native`,
+ * cpp/native.cpp) behind the same three objects — a sparse matrix (CSR), an
+ * overlap metric (Metric) and a transport engine (Engine) — with the same
+ * operations, argument meaning and error classes.  Every operation works on
+ * DEVICE buffers that the caller owns: vector blocks are row-major (N, b)
+ * arrays of complex128 (interleaved re/im doubles, b contiguous per row),
+ * exactly the layout of the reference's `Dense` (cpp/native.cpp:26-41).
+ * Matrices are passed once, as host CSR arrays, and are uploaded and owned by
+ * the library.  Work is queued on the caller's CUDA stream (`stream` is a
+ * cudaStream_t passed as void*; NULL = legacy default stream).  The engine
+ * operations and kmsd_metric_solve end with ONE synchronisation of that
+ * stream to read the device status word (failed solve acceptance, nonfinite
+ * propagation), so they return only when their results are ready; the
+ * functions documented as asynchronous do not synchronise.
+ *
+ * Return value of every int function: KMSD_OK or an error class.  The message
+ * of the last error on the calling thread is returned by kmsd_last_error().
+ * Error classes mirror the reference's exceptions:
+ *   KMSD_EINVAL   std::invalid_argument  -> ValueError        (native.cpp:33,63,316,...)
+ *   KMSD_ERUNTIME std::runtime_error     -> RuntimeError      (native.cpp:571)
+ *   KMSD_EMETRIC  MetricFailure          -> RuntimeError with per-column
+ *                                           diagnostics       (native.cpp:139-143,447-450)
+ *   KMSD_ECUDA    CUDA runtime failure (no reference counterpart)
+ *
+ * Handles are not thread-safe: one call at a time per handle (each handle owns
+ * its device workspace).  Different handles may be used concurrently.
+ */
+#ifndef KMSD_H
+#define KMSD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KMSD_OK 0
+#define KMSD_EINVAL 1
+#define KMSD_ERUNTIME 2
+#define KMSD_EMETRIC 3
+#define KMSD_ECUDA 4
+
+/* Arithmetic of an engine (kmsd_engine_create).  FP64: complex128 vectors and
+ * SpMM, the reference's precision.  MIXED: complex64 vectors and SpMM inside
+ * the Chebyshev recurrences; moment/correlation accumulation, metric solves,
+ * inner products and norms stay FP64.  Inputs and outputs are complex128 in
+ * both modes. */
+#define KMSD_FP64 0
+#define KMSD_MIXED 1
+
+/* kmsd_engine_moments flags. */
+#define KMSD_MOMENTS_DIRECT 0   /* mu_k = Re<S B, T_k B>, one operator application per moment */
+#define KMSD_MOMENTS_DOUBLING 1 /* mu_2n = 2<T_n,S T_n>-mu_0, mu_2n+1 = 2<T_n+1,S T_n>-mu_1 (S = I only) */
+
+typedef struct kmsd_csr_s *kmsd_csr;
+typedef struct kmsd_metric_s *kmsd_metric;
+typedef struct kmsd_engine_s *kmsd_engine;
+
+/* Per-column report of one metric solve; arrays of length b, caller-allocated
+ * HOST memory.  Mirrors SolveReport (cpp/native.cpp:123-129) and the Python
+ * MetricSolveReport (src/kubo_msd/contracts.py:33-39). */
+typedef struct {
+    uint8_t *converged;
+    uint8_t *breakdown;
+    int64_t *iterations;
+    double *true_residual;
+    double *relative_residual;
+} kmsd_solve_report;
+
+/* Cumulative metric counters; mirrors Metric::diagnostics
+ * (cpp/native.cpp:666-675). */
+typedef struct {
+    int64_t calls;
+    int64_t max_iterations_sum;
+    double seconds;
+    double max_relative_residual;
+    int64_t true_residual_refreshes;
+    int64_t true_residual_checks;
+    int64_t residual_restarts;
+    int64_t refinement_steps;
+} kmsd_metric_stats;
+
+/* ---- library ---------------------------------------------------------- */
+
+/* Thread-local message of the last failed call ("" if none). */
+const char *kmsd_last_error(void);
+
+/* Static description (language, precision, architecture); mirrors
+ * `_native.build_info()` (cpp/native.cpp:631-639). */
+const char *kmsd_build_info(void);
+
+/* Device ordinal the library will use (the caller's current device). */
+int kmsd_device(int *device);
+
+/* Number of kernels this library has launched in the process so far (all
+ * devices).  No counterpart in the reference; used to account the work of a
+ * timed region. */
+int64_t kmsd_kernel_launches(void);
+
+/* ---- CSR: replaces `_native.CSR` (cpp/native.cpp:54-90, 640-646) -------- */
+
+/* n rows, n columns; indptr[n+1], indices[nnz] (int64, host, 0-based);
+ * values: val_re[nnz] and val_im[nnz] (val_im NULL for a real matrix).
+ * Validation follows the reference constructor (cpp/native.cpp:59-74):
+ * monotone pointers starting at 0 and ending at nnz, indices in [0,n),
+ * finite entries; otherwise KMSD_EINVAL "invalid CSR ...".  Rows need not be
+ * sorted; entries are applied in the given order. */
+int kmsd_csr_create(int64_t n, const int64_t *indptr, const int64_t *indices,
+                    const double *val_re, const double *val_im, kmsd_csr *out);
+void kmsd_csr_destroy(kmsd_csr a);
+int64_t kmsd_csr_rows(kmsd_csr a);
+int64_t kmsd_csr_nnz(kmsd_csr a);
+
+/* Y = A X for device complex128 X, Y of shape (n, b).  Replaces CSR::mul /
+ * `CSR.matmul` (cpp/native.cpp:75-89, 642-646).  X and Y must not overlap. */
+int kmsd_csr_matmul(kmsd_csr a, const void *x, void *y, int64_t b, void *stream);
+
+/* ---- Metric: replaces `_native.Metric` (cpp/native.cpp:150-480, 647-675) */
+
+/* S: overlap (kept by reference; destroy the metric before S).
+ * diag[n] > 0: the preconditioner diagonal (positive, finite).
+ * Block-Jacobi factors (optional, nblocks = 0 for the diagonal
+ * preconditioner): block i covers rows [block_start[i], block_start[i+1]),
+ * block_start[0] = 0, block_start[nblocks] = n, each block at most 32 rows;
+ * its lower Cholesky factor is stored row-major at factor_offset[i] in
+ * factor_re/factor_im (m*m entries).  Mirrors Metric(S, diagonal, blocks)
+ * (cpp/native.cpp:212-236) and its "invalid block-Jacobi factor partition" /
+ * "incomplete block-Jacobi partition" checks. */
+int kmsd_metric_create(kmsd_csr s, const double *diag, int64_t nblocks,
+                       const int64_t *block_start, const int64_t *factor_offset,
+                       const double *factor_re, const double *factor_im,
+                       kmsd_metric *out);
+void kmsd_metric_destroy(kmsd_metric m);
+
+/* policy 0 = fixed, 1 = adaptive; interval >= 1; 0 < gap_ratio < 1.
+ * Replaces Metric::set_residual_policy (cpp/native.cpp:206-210). */
+int kmsd_metric_set_residual_policy(kmsd_metric m, int policy, int interval,
+                                    double gap_ratio);
+
+/* Y = S^-1 B by batched preconditioned CG, one independent recurrence per
+ * column, with the reference's per-column RHS scaling, thresholds
+ * max(rtol*||q||, atol/safe), curvature-breakdown test, true-residual refresh
+ * every `interval` iterations, final true-residual acceptance and
+ * representability checks (Metric::solve, cpp/native.cpp:313-452).
+ * Synchronises the stream once to read the per-column status.  On failure
+ * returns KMSD_EMETRIC with the reference's message and fills `report`
+ * (which may be NULL when not wanted). */
+int kmsd_metric_solve(kmsd_metric m, const void *b_in, void *y_out, int64_t b,
+                      double rtol, double atol, int maxiter,
+                      kmsd_solve_report *report, void *stream);
+
+/* out = D^-1/2 p(W) xi with W = (D^-1/2 S D^-1/2 - center)/half and p the
+ * Chebyshev series `coeff` (Clenshaw).  Replaces Metric::sample
+ * (cpp/native.cpp:453-479). */
+int kmsd_metric_sample(kmsd_metric m, const void *xi, void *out, int64_t b,
+                       const double *coeff, int64_t ncoeff, double center,
+                       double half, void *stream);
+
+/* Read the cumulative counters (synchronises the device). */
+int kmsd_metric_stats_get(kmsd_metric m, kmsd_metric_stats *out);
+
+/* 1 when S is exactly the identity and the preconditioner is the unit
+ * diagonal: solves are then exact copies and the engine skips them. */
+int kmsd_metric_is_identity(kmsd_metric m);
+
+/* ---- Engine: replaces `_native.Engine` (cpp/native.cpp:488-610, 676-719) */
+
+/* h: Hamiltonian; m: metric (same n).  vel_kind[3] for axes x,y,z:
+ * -1 absent, 0 explicit covariant velocity (1 matrix), 1 position
+ * (1 matrix), 2 composite bond/xbar/delta (3 matrices); vel[3*axis+j] are
+ * the matrices (NULL where unused).  rtol/atol/maxiter: metric-solve
+ * controls used inside every operator application; hbar in eV*fs.
+ * precision: KMSD_FP64 or KMSD_MIXED.  Mirrors the Engine constructor
+ * (cpp/native.cpp:495-503). */
+int kmsd_engine_create(kmsd_csr h, kmsd_metric m, const int *vel_kind,
+                       const kmsd_csr *vel, double rtol, double atol,
+                       int maxiter, double hbar, int precision,
+                       kmsd_engine *out);
+void kmsd_engine_destroy(kmsd_engine e);
+
+/* out = S^-1 H B.  Engine::h_action (cpp/native.cpp:505). */
+int kmsd_engine_h_action(kmsd_engine e, const void *b_in, void *out, int64_t b,
+                         void *stream);
+
+/* out = sum_a direction[a] v_a B with v_a the covariant Cartesian velocity of
+ * kind 0/1/2.  maxiter < 1 uses the engine's solve controls; otherwise
+ * rtol/atol/maxiter override them for this call only (v_cov_with_controls).
+ * Engine::v_cart / v_cov (cpp/native.cpp:506-533, 683-697). */
+int kmsd_engine_v_cov(kmsd_engine e, const double *direction, const void *b_in,
+                      void *out, int64_t b, double rtol, double atol,
+                      int maxiter, void *stream);
+
+/* out = sum_k coeff[k] T_k(A) B, A the augmented scaled operator of
+ * Engine::augmented: for ndir direction rows (ndir*3 doubles), B has
+ * b = nb*(1+ndir) columns [psi | phi_1..phi_ndir] and
+ * A[psi; phi_a] = [Ht psi; Ht phi_a + (-i hbar/half) S^-1 v_cov(dir_a, psi)],
+ * Ht = (S^-1 H - center)/half.  coeff: ncoeff complex values as interleaved
+ * (re, im) doubles.  Engine::series (cpp/native.cpp:540-573); fails with
+ * KMSD_ERUNTIME "nonfinite Chebyshev propagation; check bounds and solves". */
+int kmsd_engine_series(kmsd_engine e, const void *b_in, void *out, int64_t b,
+                       const double *coeff, int64_t ncoeff, double center,
+                       double half, const double *directions, int64_t ndir,
+                       void *stream);
+
+/* out[k] = T_k(Ht) B for k < length; out is (length, n, b) complex128.
+ * Engine::chain (cpp/native.cpp:574-589). */
+int kmsd_engine_chain(kmsd_engine e, const void *b_in, void *out, int64_t b,
+                      int64_t length, double center, double half, void *stream);
+
+/* mu[k*b + j] = Re sum_i conj((S B)_ij) (T_k(Ht) B)_ij for k < length, on the
+ * device (float64, (length, b)).  Engine::moments (cpp/native.cpp:590-609).
+ * flags: KMSD_MOMENTS_DIRECT or KMSD_MOMENTS_DOUBLING (S = I only). */
+int kmsd_engine_moments(kmsd_engine e, const void *b_in, double *mu, int64_t b,
+                        int64_t length, double center, double half, int flags,
+                        void *stream);
+
+/* Reference counters h_calls / v_calls (cpp/native.cpp:718-719). */
+int kmsd_engine_counters(kmsd_engine e, int64_t *h_calls, int64_t *v_calls);
+
+/* Per-column diagnostics of the metric solve that made the last engine call
+ * fail with KMSD_EMETRIC (the first failing solve of that call); the
+ * reference attaches the same dict to its MetricFailure
+ * (cpp/native.cpp:622-629, src/kubo_msd/backends/native.py:32-39).  Writes
+ * at most `capacity` columns and their count to *ncols (host memory). */
+int kmsd_engine_failure_report(kmsd_engine e, kmsd_solve_report *report,
+                               int64_t capacity, int64_t *ncols);
+
+/* out[j] = sum_i conj(A_ij) (S B)_ij, complex, into device memory as b
+ * interleaved (re, im) doubles; asynchronous.  The device form of
+ * OperatorBundle.inner (src/kubo_msd/operators/velocity.py:117), which the
+ * reference evaluates with NumPy on the host. */
+int kmsd_engine_inner(kmsd_engine e, const void *a, const void *b_in, void *out,
+                      int64_t b, void *stream);
+
+/* out[j] = sum_i conj(x_ij) y_ij for device complex128 (n, b) arrays, into
+ * device memory (b complex values); deterministic order; asynchronous.  No
+ * counterpart in the reference (its column sums run in NumPy). */
+int kmsd_column_dot(const void *x, const void *y, int64_t n, int64_t b,
+                    void *out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KMSD_H */

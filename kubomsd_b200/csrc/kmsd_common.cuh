@@ -1,0 +1,234 @@
+// Shared device/host definitions of the B200 stochastic-KPM engine.
+//
+// Vector blocks are row-major (N, b) complex arrays (the layout of the
+// reference's Dense, cpp/native.cpp:26-41).  Device code moves them in
+// 16-byte "units": one complex128 (double2) or two complex64 (float4), so
+// every global access is a 128-bit load or store.  A row of b columns is
+// U = b / C units; a "row group" of G threads (G = next power of two >= U,
+// at most 32) walks rows with a grid stride, each lane owning the units
+// lane, lane + G, ... of the row.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+namespace kmsd {
+
+// ---------------------------------------------------------------- units
+template <class T> struct Unit;
+template <> struct Unit<double> {
+    using vec = double2;
+    static constexpr int C = 1;  // complex numbers per unit
+};
+template <> struct Unit<float> {
+    using vec = float4;
+    static constexpr int C = 2;
+};
+
+// C complex numbers of precision T held in registers.
+template <class T> struct Pk {
+    static constexpr int C = Unit<T>::C;
+    T re[C], im[C];
+};
+
+__device__ __forceinline__ Pk<double> ld(const double2 *p) {
+    double2 v = *p;
+    Pk<double> r;
+    r.re[0] = v.x; r.im[0] = v.y;
+    return r;
+}
+__device__ __forceinline__ Pk<float> ld(const float4 *p) {
+    float4 v = *p;
+    Pk<float> r;
+    r.re[0] = v.x; r.im[0] = v.y; r.re[1] = v.z; r.im[1] = v.w;
+    return r;
+}
+// Read-only (non-coherent) path for gathered operands.
+__device__ __forceinline__ Pk<double> ldg(const double2 *p) {
+    double2 v = __ldg(p);
+    Pk<double> r;
+    r.re[0] = v.x; r.im[0] = v.y;
+    return r;
+}
+__device__ __forceinline__ Pk<float> ldg(const float4 *p) {
+    float4 v = __ldg(p);
+    Pk<float> r;
+    r.re[0] = v.x; r.im[0] = v.y; r.re[1] = v.z; r.im[1] = v.w;
+    return r;
+}
+__device__ __forceinline__ void st(double2 *p, const Pk<double> &a) {
+    *p = make_double2(a.re[0], a.im[0]);
+}
+__device__ __forceinline__ void st(float4 *p, const Pk<float> &a) {
+    *p = make_float4(a.re[0], a.im[0], a.re[1], a.im[1]);
+}
+
+template <class T> __device__ __forceinline__ Pk<T> pk_zero() {
+    Pk<T> r;
+#pragma unroll
+    for (int c = 0; c < Pk<T>::C; ++c) { r.re[c] = T(0); r.im[c] = T(0); }
+    return r;
+}
+
+// CSR matrix on the device with values in the vector precision T.
+template <class T> struct CsrView {
+    const int *ptr;
+    const int *idx;
+    const T *re;
+    const T *im;  // nullptr for a real matrix
+};
+
+// ---------------------------------------------------------------- mapping
+struct RowMap {
+    int G;      // threads per row group (power of two, <= 32)
+    int gpc;    // row groups per CTA
+    int U;      // units per row
+};
+
+inline int next_pow2(int x) {
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+inline RowMap make_map(int U, int threads) {
+    RowMap m;
+    m.U = U;
+    m.G = U >= 32 ? 32 : next_pow2(U < 1 ? 1 : U);
+    m.gpc = threads / m.G;
+    return m;
+}
+
+// ---------------------------------------------------------------- reductions
+// Column reductions are deterministic: a fixed grid, fixed row ownership, a
+// fixed-order shared-memory combination inside each CTA, and a fixed-order
+// combination of the per-CTA partials by the last CTA to finish (found with
+// an atomic ticket; no spinning on other CTAs).
+struct Ticket {
+    unsigned int count;
+};
+
+// Each thread holds `acc[m][c]` for its units u = lane + m*G (m < MU) and the
+// C columns of each unit.  Writes the CTA's per-column sums to
+// partial[blockIdx.x * ncol + col].  smem needs gpc * U * C double2.
+template <int MU, int C>
+__device__ __forceinline__ void cta_column_sums(const double2 (&acc)[MU][C], const RowMap &mp,
+                                                int ncol, double2 *smem, double2 *partial) {
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    if (g < mp.gpc) {
+#pragma unroll
+        for (int m = 0; m < MU; ++m) {
+            const int u = lane + m * mp.G;
+            if (u < mp.U) {
+#pragma unroll
+                for (int c = 0; c < C; ++c) smem[(g * mp.U + u) * C + c] = acc[m][c];
+            }
+        }
+    }
+    __syncthreads();
+    for (int col = threadIdx.x; col < ncol; col += blockDim.x) {
+        double sx = 0., sy = 0.;
+        for (int gg = 0; gg < mp.gpc; ++gg) {
+            const double2 v = smem[gg * mp.U * C + col];
+            sx += v.x;
+            sy += v.y;
+        }
+        partial[(size_t)blockIdx.x * ncol + col] = make_double2(sx, sy);
+    }
+    __syncthreads();
+}
+
+// Same for a max reduction of one double per column.
+template <int MU, int C>
+__device__ __forceinline__ void cta_column_max(const double (&acc)[MU][C], const RowMap &mp, int ncol,
+                                               double *smem, double *partial) {
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    if (g < mp.gpc) {
+#pragma unroll
+        for (int m = 0; m < MU; ++m) {
+            const int u = lane + m * mp.G;
+            if (u < mp.U) {
+#pragma unroll
+                for (int c = 0; c < C; ++c) smem[(g * mp.U + u) * C + c] = acc[m][c];
+            }
+        }
+    }
+    __syncthreads();
+    for (int col = threadIdx.x; col < ncol; col += blockDim.x) {
+        double s = 0.;
+        for (int gg = 0; gg < mp.gpc; ++gg) s = fmax(s, smem[gg * mp.U * C + col]);
+        partial[(size_t)blockIdx.x * ncol + col] = s;
+    }
+    __syncthreads();
+}
+
+// Returns true in exactly one CTA (the last to arrive), after all other CTAs'
+// partials are visible.  Resets the ticket for the next launch.
+__device__ __forceinline__ bool last_cta(Ticket *t) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned prev = atomicAdd(&t->count, 1u);
+        is_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (is_last) {
+        __threadfence();
+        if (threadIdx.x == 0) t->count = 0;
+    }
+    return is_last;
+}
+
+// Inside the last CTA: out[col] = sum over CTAs (fixed order) of partial.
+// Uses all threads: the CTAs are split into `split` fixed contiguous ranges
+// per column, combined in a fixed order through shared memory.
+__device__ __forceinline__ void final_column_sums(const double2 *partial, int nparts, int ncol,
+                                                  double2 *smem /* blockDim.x */, double2 *out) {
+    // Process columns in chunks of at most blockDim.x.
+    for (int c0 = 0; c0 < ncol; c0 += blockDim.x) {
+        const int cols = min((int)blockDim.x, ncol - c0);
+        const int split = max(1, (int)blockDim.x / cols);
+        const int col = threadIdx.x % cols, part = threadIdx.x / cols;
+        double sx = 0., sy = 0.;
+        if (part < split) {
+            const int per = (nparts + split - 1) / split;
+            const int lo = part * per, hi = min(nparts, lo + per);
+            for (int p = lo; p < hi; ++p) {
+                const double2 v = __ldcg(partial + (size_t)p * ncol + c0 + col);
+                sx += v.x;
+                sy += v.y;
+            }
+        }
+        __syncthreads();
+        if (part < split) smem[part * cols + col] = make_double2(sx, sy);
+        __syncthreads();
+        if (threadIdx.x < cols) {
+            double tx = 0., ty = 0.;
+            for (int p = 0; p < split; ++p) {
+                const double2 v = smem[p * cols + threadIdx.x];
+                tx += v.x;
+                ty += v.y;
+            }
+            out[c0 + threadIdx.x] = make_double2(tx, ty);
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void final_column_max(const double *partial, int nparts, int ncol,
+                                                 double *out) {
+    for (int col = threadIdx.x; col < ncol; col += blockDim.x) {
+        double s = 0.;
+        for (int p = 0; p < nparts; ++p) s = fmax(s, __ldcg(partial + (size_t)p * ncol + col));
+        out[col] = s;
+    }
+}
+
+// ---------------------------------------------------------------- host errors
+struct Error {
+    int code;
+    std::string msg;
+};
+
+}  // namespace kmsd

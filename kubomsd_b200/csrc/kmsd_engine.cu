@@ -1,0 +1,344 @@
+// Transport engine of the B200 stochastic-KPM backend: sparse matrices, the
+// operator applications of the reference Engine (cpp/native.cpp:488-610) and
+// the C ABI around them.
+//
+// Two execution paths:
+//  * identity metric (orthogonal basis, S = I with unit diagonal): every
+//    Chebyshev step is ONE fused kernel (cheb_step_kernel) that streams the
+//    vector block once — SpMM of H, spectral rescaling, three-term recurrence,
+//    velocity injection and the moment / series epilogue — in FP64 or in the
+//    mixed form (complex64 vectors, FP64 accumulations);
+//  * general metric: H X (SpMM), S^-1 by the batched PCG of kmsd_metric.cu,
+//    then the same step kernel reading the solved operand (FP64 only).
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <utility>
+#include <vector>
+
+#include "kmsd.h"
+#include "kmsd_impl.h"
+#include "kmsd_kernels.cuh"
+
+using namespace kmsd;
+
+// ------------------------------------------------------------------ errors
+namespace {
+thread_local std::string g_last_error;
+}
+namespace kmsd {
+int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+int cuda_fail(cudaError_t e, const char *what) {
+    g_last_error = std::string("CUDA error ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ") in " + what;
+    return KMSD_ECUDA;
+}
+int DevBuf::ensure(size_t want) {
+    if (want <= bytes && p) return 0;
+    release();
+    if (want == 0) want = 16;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        bytes = 0;
+        cuda_fail(e, "cudaMalloc (workspace)");
+        return 1;
+    }
+    bytes = want;
+    return 0;
+}
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+static std::atomic<int64_t> g_launches{0};
+void count_launch(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+int64_t launches() { return g_launches.load(std::memory_order_relaxed); }
+int sm_count() {
+    static int cached = 0;
+    if (!cached) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, dev);
+        if (cached <= 0) cached = 148;
+    }
+    return cached;
+}
+int grid_for(int64_t rows, const RowMap &mp) {
+    const int64_t need = (rows + mp.gpc - 1) / mp.gpc;
+    const int64_t cap = (int64_t)sm_count() * 8;  // 8 CTAs of 256 threads per SM
+    return (int)std::max<int64_t>(1, std::min(need, cap));
+}
+int mu_for(const RowMap &mp) {
+    const int per = (mp.U + mp.G - 1) / mp.G;
+    if (per <= 1) return 1;
+    if (per <= 2) return 2;
+    if (per <= 4) return 4;
+    if (per <= 8) return 8;
+    return 0;
+}
+size_t reduce_smem(const RowMap &mp, int C) {
+    const size_t a = (size_t)mp.gpc * mp.U * C, b = kThreads;
+    return std::max(a, b) * sizeof(double2);
+}
+int Reducer::ensure(int grid, int ncol, int copies) {
+    if (partial.ensure((size_t)grid * ncol * copies * sizeof(double2) + 64)) return KMSD_ECUDA;
+    if (!ticket.p) {
+        if (ticket.ensure(64)) return KMSD_ECUDA;
+        KMSD_CUDA(cudaMemset(ticket.p, 0, 64));
+    }
+    return KMSD_OK;
+}
+}  // namespace kmsd
+
+// ------------------------------------------------------------------ CSR
+int kmsd_csr_s::ensure_f32() {
+    if (re32) return KMSD_OK;
+    std::vector<double> h(nnz);
+    std::vector<float> f(nnz);
+    KMSD_CUDA(cudaMemcpy(h.data(), re64, nnz * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < nnz; ++i) f[i] = (float)h[i];
+    KMSD_CUDA(cudaMalloc(&re32, std::max<int64_t>(nnz, 1) * sizeof(float)));
+    KMSD_CUDA(cudaMemcpy(re32, f.data(), nnz * sizeof(float), cudaMemcpyHostToDevice));
+    if (complex_values) {
+        KMSD_CUDA(cudaMemcpy(h.data(), im64, nnz * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < nnz; ++i) f[i] = (float)h[i];
+        KMSD_CUDA(cudaMalloc(&im32, std::max<int64_t>(nnz, 1) * sizeof(float)));
+        KMSD_CUDA(cudaMemcpy(im32, f.data(), nnz * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    return KMSD_OK;
+}
+
+namespace {
+template <class T, int MU, bool DOT>
+void launch_spmm(CsrView<T> A, const typename Unit<T>::vec *X, typename Unit<T>::vec *Y, int64_t n, RowMap mp,
+                 Reducer &red, double2 *dot, cudaStream_t s) {
+    const int grid = grid_for(n, mp);
+    spmm_kernel<T, MU, DOT><<<grid, kThreads, reduce_smem(mp, Unit<T>::C), s>>>(A, X, Y, n, mp, red.part(),
+                                                                               red.tick(), dot);
+    count_launch();
+}
+template <class T>
+int spmm_any(CsrView<T> A, const typename Unit<T>::vec *X, typename Unit<T>::vec *Y, int64_t n, int U,
+             cudaStream_t s, double2 *dot) {
+    static thread_local Reducer red;
+    const RowMap mp = make_map(U, kThreads);
+    const int mu = mu_for(mp);
+    if (!mu) return fail(KMSD_EINVAL, "too many columns for one SpMM call");
+    if (red.ensure(grid_for(n, mp), U * Unit<T>::C)) return KMSD_ECUDA;
+#define KMSD_SPMM_CASE(M)                                                      \
+    case M:                                                                    \
+        if (dot) launch_spmm<T, M, true>(A, X, Y, n, mp, red, dot, s);         \
+        else launch_spmm<T, M, false>(A, X, Y, n, mp, red, nullptr, s);        \
+        break;
+    switch (mu) {
+        KMSD_SPMM_CASE(1)
+        KMSD_SPMM_CASE(2)
+        KMSD_SPMM_CASE(4)
+        KMSD_SPMM_CASE(8)
+    }
+#undef KMSD_SPMM_CASE
+    KMSD_CUDA(cudaGetLastError());
+    return KMSD_OK;
+}
+}  // namespace
+
+namespace kmsd {
+int spmm64(const kmsd_csr_s *A, const double2 *X, double2 *Y, int64_t b, cudaStream_t s, double2 *dot_out) {
+    return spmm_any<double>(A->view64(), X, Y, A->n, (int)b, s, dot_out);
+}
+int spmm32(const kmsd_csr_s *A, const float4 *X, float4 *Y, int64_t U, cudaStream_t s, double2 *dot_out) {
+    return spmm_any<float>(A->view32(), X, Y, A->n, (int)U, s, dot_out);
+}
+int lincomb(cudaStream_t s, double2 *y, int64_t len, int accumulate, int terms, const double2 *const *x,
+            const double *cr, const double *ci) {
+    Lincomb L{};
+    L.terms = terms;
+    L.accumulate = accumulate;
+    for (int t = 0; t < terms; ++t) {
+        L.x[t] = x[t];
+        L.cr[t] = cr[t];
+        L.ci[t] = ci[t];
+    }
+    const int grid = (int)std::min<int64_t>((len + 255) / 256, (int64_t)sm_count() * 16);
+    lincomb_kernel<<<std::max(grid, 1), 256, 0, s>>>(L, y, len);
+    count_launch();
+    KMSD_CUDA(cudaGetLastError());
+    return KMSD_OK;
+}
+}  // namespace kmsd
+
+// ------------------------------------------------------------------ column dot
+namespace {
+// out[j] = sum_i conj(x_ij) y_ij (complex, double2), deterministic.
+template <class T, int MU>
+__global__ void __launch_bounds__(256) coldot_kernel(const typename Unit<T>::vec *x, const typename Unit<T>::vec *y,
+                                                     int64_t n, RowMap mp, double2 *partial, Ticket *tk,
+                                                     double2 *out) {
+    constexpr int C = Unit<T>::C;
+    extern __shared__ double2 smem[];
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    double2 acc[MU][C];
+#pragma unroll
+    for (int m = 0; m < MU; ++m)
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[m][c] = make_double2(0., 0.);
+    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < n; row += (int64_t)gridDim.x * mp.gpc) {
+#pragma unroll
+        for (int m = 0; m < MU; ++m) {
+            const int u = lane + m * mp.G;
+            if (u < mp.U) {
+                const size_t o = (size_t)row * mp.U + u;
+                const Pk<T> a = ld(x + o), b = ld(y + o);
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    acc[m][c].x += (double)a.re[c] * b.re[c] + (double)a.im[c] * b.im[c];
+                    acc[m][c].y += (double)a.re[c] * b.im[c] - (double)a.im[c] * b.re[c];
+                }
+            }
+        }
+    }
+    const int ncol = mp.U * C;
+    cta_column_sums<MU, C>(acc, mp, ncol, smem, partial);
+    if (last_cta(tk)) final_column_sums(partial, gridDim.x, ncol, smem, out);
+}
+
+template <class T>
+int coldot_any(const typename Unit<T>::vec *x, const typename Unit<T>::vec *y, int64_t n, int U, double2 *out,
+               cudaStream_t s) {
+    static thread_local Reducer red;
+    const RowMap mp = make_map(U, kThreads);
+    const int mu = mu_for(mp);
+    if (!mu) return fail(KMSD_EINVAL, "too many columns for one reduction");
+    const int grid = grid_for(n, mp);
+    if (red.ensure(grid, U * Unit<T>::C)) return KMSD_ECUDA;
+    const size_t sm = reduce_smem(mp, Unit<T>::C);
+    switch (mu) {
+        case 1: coldot_kernel<T, 1><<<grid, kThreads, sm, s>>>(x, y, n, mp, red.part(), red.tick(), out); break;
+        case 2: coldot_kernel<T, 2><<<grid, kThreads, sm, s>>>(x, y, n, mp, red.part(), red.tick(), out); break;
+        case 4: coldot_kernel<T, 4><<<grid, kThreads, sm, s>>>(x, y, n, mp, red.part(), red.tick(), out); break;
+        case 8: coldot_kernel<T, 8><<<grid, kThreads, sm, s>>>(x, y, n, mp, red.part(), red.tick(), out); break;
+    }
+    count_launch();
+    KMSD_CUDA(cudaGetLastError());
+    return KMSD_OK;
+}
+
+__global__ void take_real_kernel(const double2 *src, double *dst, int n) {
+    for (int j = threadIdx.x; j < n; j += blockDim.x) dst[j] = src[j].x;
+}
+}  // namespace
+
+namespace kmsd {
+int coldot64(const double2 *x, const double2 *y, int64_t n, int64_t b, double2 *out, cudaStream_t s) {
+    return coldot_any<double>(x, y, n, (int)b, out, s);
+}
+int coldot32(const float4 *x, const float4 *y, int64_t n, int64_t U, double2 *out, cudaStream_t s) {
+    return coldot_any<float>(x, y, n, (int)U, out, s);
+}
+int take_real(const double2 *src, double *dst, int64_t b, cudaStream_t s) {
+    take_real_kernel<<<1, 256, 0, s>>>(src, dst, (int)b);
+    count_launch();
+    KMSD_CUDA(cudaGetLastError());
+    return KMSD_OK;
+}
+}  // namespace kmsd
+
+// ------------------------------------------------------------------ CSR ABI
+extern "C" {
+
+const char *kmsd_last_error(void) { return g_last_error.c_str(); }
+
+int64_t kmsd_kernel_launches(void) { return launches(); }
+
+const char *kmsd_build_info(void) {
+    return "{\"language\": \"C++17/CUDA\", \"architecture\": \"sm_100a\", "
+           "\"precision\": \"complex128/float64 (FP64) or complex64 vectors with float64 accumulation (MIXED)\", "
+           "\"implementation\": \"fused CSR SpMM + Chebyshev recurrence kernels, batched device PCG\"}";
+}
+
+int kmsd_device(int *device) {
+    if (!device) return fail(KMSD_EINVAL, "null device pointer");
+    KMSD_CUDA(cudaGetDevice(device));
+    return KMSD_OK;
+}
+
+int kmsd_csr_create(int64_t n, const int64_t *indptr, const int64_t *indices, const double *val_re,
+                    const double *val_im, kmsd_csr *out) {
+    if (!out || n < 1 || !indptr) return fail(KMSD_EINVAL, "invalid CSR dimensions/threads");
+    const int64_t nnz = indptr[n];
+    if (indptr[0] != 0 || nnz < 0) return fail(KMSD_EINVAL, "invalid CSR row pointers");
+    if (nnz > 0 && (!indices || !val_re)) return fail(KMSD_EINVAL, "invalid CSR dimensions/threads");
+    for (int64_t r = 0; r < n; ++r)
+        if (indptr[r] > indptr[r + 1]) return fail(KMSD_EINVAL, "nonmonotone CSR row pointers");
+    for (int64_t k = 0; k < nnz; ++k)
+        if (indices[k] < 0 || indices[k] >= n || !std::isfinite(val_re[k]) ||
+            (val_im && !std::isfinite(val_im[k])))
+            return fail(KMSD_EINVAL, "invalid CSR index or nonfinite entry");
+    if (n >= INT32_MAX || nnz >= INT32_MAX) return fail(KMSD_EINVAL, "CSR too large for 32-bit indices");
+    bool cplx = false;
+    if (val_im)
+        for (int64_t k = 0; k < nnz && !cplx; ++k) cplx = val_im[k] != 0.;
+    bool ident = nnz == n;
+    for (int64_t r = 0; r < n && ident; ++r)
+        ident = indptr[r] == r && indices[r] == r && val_re[r] == 1. && (!val_im || val_im[r] == 0.);
+    std::vector<int> p32(n + 1), i32(std::max<int64_t>(nnz, 1));
+    for (int64_t r = 0; r <= n; ++r) p32[r] = (int)indptr[r];
+    for (int64_t k = 0; k < nnz; ++k) i32[k] = (int)indices[k];
+    auto *A = new kmsd_csr_s();
+    A->n = n;
+    A->nnz = nnz;
+    A->complex_values = cplx;
+    A->identity = ident;
+    cudaGetDevice(&A->device);
+    auto up = [&](void **dst, const void *src, size_t bytes) -> int {
+        KMSD_CUDA(cudaMalloc(dst, std::max<size_t>(bytes, 16)));
+        if (bytes) KMSD_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+        return KMSD_OK;
+    };
+    int rc = up((void **)&A->ptr, p32.data(), (n + 1) * sizeof(int));
+    if (!rc) rc = up((void **)&A->idx, i32.data(), nnz * sizeof(int));
+    if (!rc) rc = up((void **)&A->re64, val_re, nnz * sizeof(double));
+    if (!rc && cplx) rc = up((void **)&A->im64, val_im, nnz * sizeof(double));
+    if (rc) {
+        kmsd_csr_destroy(A);
+        return rc;
+    }
+    *out = A;
+    return KMSD_OK;
+}
+
+void kmsd_csr_destroy(kmsd_csr a) {
+    if (!a) return;
+    cudaFree(a->ptr);
+    cudaFree(a->idx);
+    cudaFree(a->re64);
+    cudaFree(a->im64);
+    cudaFree(a->re32);
+    cudaFree(a->im32);
+    delete a;
+}
+
+int64_t kmsd_csr_rows(kmsd_csr a) { return a ? a->n : -1; }
+int64_t kmsd_csr_nnz(kmsd_csr a) { return a ? a->nnz : -1; }
+
+int kmsd_csr_matmul(kmsd_csr a, const void *x, void *y, int64_t b, void *stream) {
+    if (!a || !x || !y || b < 1) return fail(KMSD_EINVAL, "CSR input dimension mismatch");
+    return spmm64(a, static_cast<const double2 *>(x), static_cast<double2 *>(y), b,
+                  static_cast<cudaStream_t>(stream));
+}
+
+int kmsd_column_dot(const void *x, const void *y, int64_t n, int64_t b, void *out, void *stream) {
+    if (!x || !y || !out || n < 1 || b < 1) return fail(KMSD_EINVAL, "invalid column dot dimensions");
+    return coldot64(static_cast<const double2 *>(x), static_cast<const double2 *>(y), n, b,
+                    static_cast<double2 *>(out), static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"
+

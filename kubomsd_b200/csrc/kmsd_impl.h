@@ -1,0 +1,132 @@
+// Host-side objects of libkmsd_b200.so shared by the metric and engine
+// translation units.  Not part of the public ABI (include/kmsd.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "kmsd_common.cuh"
+
+namespace kmsd {
+
+constexpr int kThreads = 256;
+
+// Last-error state (thread local) and status helpers.
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+#define KMSD_CUDA(call)                                      \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+    } while (0)
+
+// Grow-only device buffer.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t want);
+    void release();
+    template <class X> X *as() const { return static_cast<X *>(p); }
+};
+
+int sm_count();
+// Process-wide count of kernels launched by the library.
+void count_launch(int64_t n = 1);
+// Grid for a row-group kernel over `rows` rows.
+int grid_for(int64_t rows, const RowMap &mp);
+// Units per thread bucket {1,2,4,8}; 0 when too wide.
+int mu_for(const RowMap &mp);
+size_t reduce_smem(const RowMap &mp, int C);
+
+}  // namespace kmsd
+
+// ------------------------------------------------------------------ CSR
+struct kmsd_csr_s {
+    int64_t n = 0, nnz = 0;
+    int *ptr = nullptr, *idx = nullptr;
+    double *re64 = nullptr, *im64 = nullptr;
+    float *re32 = nullptr, *im32 = nullptr;  // created on first mixed use
+    bool complex_values = false;
+    bool identity = false;
+    int device = 0;
+    int ensure_f32();
+    kmsd::CsrView<double> view64() const { return {ptr, idx, re64, complex_values ? im64 : nullptr}; }
+    kmsd::CsrView<float> view32() const { return {ptr, idx, re32, complex_values ? im32 : nullptr}; }
+};
+
+namespace kmsd {
+// Y = A X over complex128 (n, b); optional curvature dot into dot_out (double2[b]).
+int spmm64(const kmsd_csr_s *A, const double2 *X, double2 *Y, int64_t b, cudaStream_t s,
+           double2 *dot_out = nullptr);
+int spmm32(const kmsd_csr_s *A, const float4 *X, float4 *Y, int64_t U, cudaStream_t s,
+           double2 *dot_out = nullptr);
+// out[j] = sum_i conj(x_ij) y_ij into device double2[ncol] (deterministic).
+int coldot64(const double2 *x, const double2 *y, int64_t n, int64_t b, double2 *out, cudaStream_t s);
+int coldot32(const float4 *x, const float4 *y, int64_t n, int64_t U, double2 *out, cudaStream_t s);
+int take_real(const double2 *src, double *dst, int64_t b, cudaStream_t s);
+// y = sum coef_m x_m  (or y += ...).
+int lincomb(cudaStream_t s, double2 *y, int64_t len, int accumulate, int terms, const double2 *const *x,
+            const double *cr, const double *ci);
+// Shared scratch for reductions (partials + tickets), grown per call site.
+struct Reducer {
+    DevBuf partial;
+    DevBuf ticket;
+    int ensure(int grid, int ncol, int copies = 1);
+    double2 *part() const { return partial.as<double2>(); }
+    Ticket *tick() const { return ticket.as<Ticket>(); }
+};
+}  // namespace kmsd
+
+// ------------------------------------------------------------------ metric
+struct PcgCols;
+struct kmsd_metric_s {
+    kmsd_csr_s *S = nullptr;
+    int64_t n = 0;
+    double *diag = nullptr;   // device
+    double *zinv = nullptr;   // 1/sqrt(diag), device (sampling)
+    int64_t nblocks = 0;      // 0: diagonal preconditioner
+    int *bstart = nullptr;    // device, nblocks+1
+    int64_t *foff = nullptr;  // device
+    double2 *factors = nullptr;
+    int maxb = 1;
+    bool identity = false;
+    int adaptive = 0, interval = 32;
+    double gap_ratio = .1;
+    // workspace
+    int64_t wb = 0;  // columns the workspace is sized for
+    kmsd::DevBuf q, y, r, z, p, sp, t;
+    kmsd::DevBuf cols;       // per-column state (PcgCols layout)
+    kmsd::DevBuf host_pinned;  // pinned host flags
+    kmsd::Reducer red;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    // counters (host side, plus device counters folded in on read)
+    int64_t calls = 0;
+    double seconds = 0.;
+    kmsd::DevBuf dcount;  // device counters: refreshes, checks, restarts, iters_sum, max_rel(bits)
+    int ensure(int64_t b);
+    // Batched PCG on device buffers (complex128).  When `report` is null and
+    // `status` non-null, the call is asynchronous: a failure is recorded in
+    // *status (first failure wins) together with the per-column report in
+    // `fail_report`.
+    int solve(const double2 *B, double2 *Y, int64_t b, double rtol, double atol, int maxiter,
+              kmsd_solve_report *report, cudaStream_t s, int *status = nullptr, void *fail_report = nullptr);
+};
+
+// Per-column device failure report for asynchronous solves.
+struct FailReport {
+    int64_t ncols;
+    int code;  // KMSD_EMETRIC / KMSD_EINVAL
+    int reason;  // 0 acceptance, 1 breakdown, 2 not representable, 3 nonfinite RHS
+};
+constexpr int kMaxReportCols = 512;
+struct FailReportFull {
+    FailReport head;
+    uint8_t converged[kMaxReportCols];
+    uint8_t breakdown[kMaxReportCols];
+    int64_t iterations[kMaxReportCols];
+    double true_residual[kMaxReportCols];
+    double relative_residual[kMaxReportCols];
+};

@@ -1,0 +1,441 @@
+// Device kernels of the B200 stochastic-KPM engine: CSR SpMM, the fused
+// Chebyshev step (moments / chain / augmented series), the Clenshaw sampling
+// step, and small elementwise helpers.  Every kernel is a grid-stride loop
+// over row groups (RowMap) with 128-bit unit accesses; reductions go through
+// the deterministic two-stage column sums of kmsd_common.cuh.
+#pragma once
+
+#include "kmsd_common.cuh"
+
+namespace kmsd {
+
+// ------------------------------------------------------------ complex helpers
+template <class T>
+__device__ __forceinline__ void cmac_real(Pk<T> &acc, T v, const Pk<T> &x) {
+#pragma unroll
+    for (int c = 0; c < Pk<T>::C; ++c) {
+        acc.re[c] = fma(v, x.re[c], acc.re[c]);
+        acc.im[c] = fma(v, x.im[c], acc.im[c]);
+    }
+}
+template <class T>
+__device__ __forceinline__ void cmac_cplx(Pk<T> &acc, T vr, T vi, const Pk<T> &x) {
+#pragma unroll
+    for (int c = 0; c < Pk<T>::C; ++c) {
+        acc.re[c] = fma(vr, x.re[c], fma(-vi, x.im[c], acc.re[c]));
+        acc.im[c] = fma(vr, x.im[c], fma(vi, x.re[c], acc.im[c]));
+    }
+}
+// a / s for real s: IEEE division in FP64 (the reference divides by the
+// spectral half-width), multiplication by the reciprocal in FP32.
+__device__ __forceinline__ double rdiv(double a, double s, double) { return a / s; }
+__device__ __forceinline__ float rdiv(float a, float, float inv) { return a * inv; }
+
+// acc[m] += sum_k A[row,k] X[k, unit u_m]   for the MU units of this lane.
+template <class T, int MU>
+__device__ __forceinline__ void gather_row(const CsrView<T> &A, const typename Unit<T>::vec *X,
+                                           int64_t row, int U, int G, int lane, Pk<T> (&acc)[MU]) {
+    const int k0 = __ldg(A.ptr + row), k1 = __ldg(A.ptr + row + 1);
+    if (A.im == nullptr) {
+        for (int k = k0; k < k1; ++k) {
+            const int col = __ldg(A.idx + k);
+            const T v = __ldg(A.re + k);
+            const typename Unit<T>::vec *src = X + (size_t)col * U;
+#pragma unroll
+            for (int m = 0; m < MU; ++m) {
+                const int u = lane + m * G;
+                if (u < U) cmac_real(acc[m], v, ldg(src + u));
+            }
+        }
+    } else {
+        for (int k = k0; k < k1; ++k) {
+            const int col = __ldg(A.idx + k);
+            const T vr = __ldg(A.re + k), vi = __ldg(A.im + k);
+            const typename Unit<T>::vec *src = X + (size_t)col * U;
+#pragma unroll
+            for (int m = 0; m < MU; ++m) {
+                const int u = lane + m * G;
+                if (u < U) cmac_cplx(acc[m], vr, vi, ldg(src + u));
+            }
+        }
+    }
+}
+
+// Same for one unit (runtime loop callers).
+template <class T>
+__device__ __forceinline__ Pk<T> gather_unit(const CsrView<T> &A, const typename Unit<T>::vec *X,
+                                             int64_t row, int U, int u) {
+    Pk<T> acc = pk_zero<T>();
+    const int k0 = __ldg(A.ptr + row), k1 = __ldg(A.ptr + row + 1);
+    if (A.im == nullptr) {
+        for (int k = k0; k < k1; ++k)
+            cmac_real(acc, __ldg(A.re + k), ldg(X + (size_t)__ldg(A.idx + k) * U + u));
+    } else {
+        for (int k = k0; k < k1; ++k)
+            cmac_cplx(acc, __ldg(A.re + k), __ldg(A.im + k), ldg(X + (size_t)__ldg(A.idx + k) * U + u));
+    }
+    return acc;
+}
+
+// ------------------------------------------------------------ SpMM
+// Y = A X (optionally with per-column partial sums of conj(X_row) * Y_row,
+// the curvature <p, S p> of the metric solve).
+template <class T, int MU, bool DOT>
+__global__ void __launch_bounds__(256) spmm_kernel(CsrView<T> A, const typename Unit<T>::vec *X,
+                                                   typename Unit<T>::vec *Y, int64_t n, RowMap mp,
+                                                   double2 *partial, Ticket *ticket, double2 *dot_out) {
+    using V = typename Unit<T>::vec;
+    constexpr int C = Unit<T>::C;
+    extern __shared__ double2 smem[];
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    double2 acc[MU][C];
+#pragma unroll
+    for (int m = 0; m < MU; ++m)
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[m][c] = make_double2(0., 0.);
+    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < n; row += (int64_t)gridDim.x * mp.gpc) {
+        Pk<T> y[MU];
+#pragma unroll
+        for (int m = 0; m < MU; ++m) y[m] = pk_zero<T>();
+        gather_row<T, MU>(A, X, row, mp.U, mp.G, lane, y);
+#pragma unroll
+        for (int m = 0; m < MU; ++m) {
+            const int u = lane + m * mp.G;
+            if (u < mp.U) {
+                const size_t o = (size_t)row * mp.U + u;
+                st(Y + o, y[m]);
+                if (DOT) {
+                    const Pk<T> x = ld(X + o);
+#pragma unroll
+                    for (int c = 0; c < C; ++c) {
+                        // conj(x) * y
+                        acc[m][c].x += (double)x.re[c] * y[m].re[c] + (double)x.im[c] * y[m].im[c];
+                        acc[m][c].y += (double)x.re[c] * y[m].im[c] - (double)x.im[c] * y[m].re[c];
+                    }
+                }
+            }
+        }
+    }
+    if (DOT) {
+        const int ncol = mp.U * C;
+        cta_column_sums<MU, C>(acc, mp, ncol, smem, partial);
+        if (last_cta(ticket)) final_column_sums(partial, gridDim.x, ncol, smem, dot_out);
+    }
+}
+
+// ------------------------------------------------------------ Chebyshev step
+// next = first ? t : 2 t - prev,  t = (h - center x)/half  [+ injection],
+// h = S^-1 H x: computed inline from H when the metric is the identity
+// (h_inline) or read from a precomputed buffer `hx` (general metric).
+// MODE selects the epilogue:
+//   MODE_CHAIN    store next (and optionally a complex128 copy)
+//   MODE_DIRECT   moment mu_k[j] = Re sum_i conj(bra_ij) next_ij
+//   MODE_DOUBLING s_even = <x,x>, s_odd = <x,next>  (mu_2n, mu_2n+1)
+//   MODE_SERIES   out = first ? c0 x + c1 next : out + ck next, with the
+//                 augmented velocity injection on the phi columns
+enum { MODE_CHAIN = 0, MODE_DIRECT = 1, MODE_DOUBLING = 2, MODE_SERIES = 3 };
+
+template <class T> struct StepArgs {
+    using V = typename Unit<T>::vec;
+    int64_t n;
+    RowMap mp;
+    CsrView<T> H;          // inline operator (identity metric)
+    const V *hx;           // precomputed S^-1 H x (general metric), or nullptr
+    const V *curr;         // T_{k-1} (= x)
+    const V *prev;         // T_{k-2}; may alias `next`
+    V *next;               // T_k
+    int first;             // k == 1
+    double center, half;
+    T inv_half;
+    // moments
+    const V *bra;          // S B (MODE_DIRECT)
+    double2 *partial;      // [grid][ncol] (x2 for doubling)
+    Ticket *ticket;
+    double *mu;            // moment array (length, bcols)
+    int64_t kmom;          // MODE_DIRECT: row of mu; MODE_DOUBLING: n
+    int64_t mlen;          // number of moments
+    int bcols;             // real columns (<= U*C)
+    // chain copy-out (complex128), MODE_CHAIN
+    double2 *store64;
+    // series
+    V *out;
+    T c0r, c0i, ckr, cki;  // coefficients (c0 used when first)
+    int UR;                // units of the psi block (0: no augmentation)
+    int nphi;              // number of phi blocks
+    // inline velocity: for each axis, CSR and weight w[a][axis] (complex)
+    CsrView<T> Vm[3];
+    int nvel;              // number of velocity matrices in use
+    int vel_axis[3];
+    T wr[4][3], wi[4][3];  // injection weights per phi block and velocity matrix
+    // precomputed injection (general path): inj[a] of shape (n, UR units), FP64 complex
+    const V *inj[4];
+    T injr, inji;          // injection scale (-i hbar / half)
+    int *status;           // nonfinite flag for series output
+};
+
+template <class T, int MU, int MODE, bool INLINE_H, bool INLINE_V>
+__global__ void __launch_bounds__(256) cheb_step_kernel(const StepArgs<T> a) {
+    using V = typename Unit<T>::vec;
+    constexpr int C = Unit<T>::C;
+    extern __shared__ double2 smem[];
+    const RowMap mp = a.mp;
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    double2 acc0[MU][C], acc1[MU][C];
+#pragma unroll
+    for (int m = 0; m < MU; ++m)
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            acc0[m][c] = make_double2(0., 0.);
+            acc1[m][c] = make_double2(0., 0.);
+        }
+    const T cen = (T)a.center, hal = (T)a.half;
+    bool bad = false;
+    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < a.n; row += (int64_t)gridDim.x * mp.gpc) {
+        Pk<T> h[MU];
+        if (INLINE_H) {
+#pragma unroll
+            for (int m = 0; m < MU; ++m) h[m] = pk_zero<T>();
+            gather_row<T, MU>(a.H, a.curr, row, mp.U, mp.G, lane, h);
+        }
+#pragma unroll
+        for (int m = 0; m < MU; ++m) {
+            const int u = lane + m * mp.G;
+            if (u >= mp.U) continue;
+            const size_t o = (size_t)row * mp.U + u;
+            const Pk<T> x = ld(a.curr + o);
+            const Pk<T> hv = INLINE_H ? h[m] : ld(a.hx + o);
+            Pk<T> t;
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                t.re[c] = rdiv(hv.re[c] - cen * x.re[c], hal, a.inv_half);
+                t.im[c] = rdiv(hv.im[c] - cen * x.im[c], hal, a.inv_half);
+            }
+            if (MODE == MODE_SERIES && a.UR > 0 && u >= a.UR) {
+                const int blk = u / a.UR - 1;  // phi block
+                const int upsi = u - (blk + 1) * a.UR;
+                if (INLINE_V) {
+                    for (int v = 0; v < a.nvel; ++v) {
+                        const T wr = a.wr[blk][v], wi = a.wi[blk][v];
+                        if (wr == T(0) && wi == T(0)) continue;
+                        const Pk<T> vp = gather_unit<T>(a.Vm[v], a.curr, row, mp.U, upsi);
+#pragma unroll
+                        for (int c = 0; c < C; ++c) {
+                            t.re[c] += wr * vp.re[c] - wi * vp.im[c];
+                            t.im[c] += wr * vp.im[c] + wi * vp.re[c];
+                        }
+                    }
+                } else {
+                    const Pk<T> v = ld(a.inj[blk] + (size_t)row * a.UR + upsi);
+#pragma unroll
+                    for (int c = 0; c < C; ++c) {
+                        t.re[c] += a.injr * v.re[c] - a.inji * v.im[c];
+                        t.im[c] += a.injr * v.im[c] + a.inji * v.re[c];
+                    }
+                }
+            }
+            Pk<T> nx;
+            if (a.first) {
+                nx = t;
+            } else {
+                const Pk<T> p = ld(a.prev + o);
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    nx.re[c] = T(2) * t.re[c] - p.re[c];
+                    nx.im[c] = T(2) * t.im[c] - p.im[c];
+                }
+            }
+            st(a.next + o, nx);
+            if (MODE == MODE_CHAIN && a.store64 != nullptr) {
+#pragma unroll
+                for (int c = 0; c < C; ++c)
+                    a.store64[o * C + c] = make_double2((double)nx.re[c], (double)nx.im[c]);
+            }
+            if (MODE == MODE_DIRECT) {
+                const Pk<T> br = ld(a.bra + o);
+#pragma unroll
+                for (int c = 0; c < C; ++c)
+                    acc0[m][c].x += (double)br.re[c] * (double)nx.re[c] + (double)br.im[c] * (double)nx.im[c];
+            }
+            if (MODE == MODE_DOUBLING) {
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    acc0[m][c].x += (double)x.re[c] * (double)x.re[c] + (double)x.im[c] * (double)x.im[c];
+                    acc1[m][c].x += (double)x.re[c] * (double)nx.re[c] + (double)x.im[c] * (double)nx.im[c];
+                }
+            }
+            if (MODE == MODE_SERIES) {
+                Pk<T> ov;
+                if (a.first) {
+#pragma unroll
+                    for (int c = 0; c < C; ++c) {
+                        ov.re[c] = a.c0r * x.re[c] - a.c0i * x.im[c] + a.ckr * nx.re[c] - a.cki * nx.im[c];
+                        ov.im[c] = a.c0r * x.im[c] + a.c0i * x.re[c] + a.ckr * nx.im[c] + a.cki * nx.re[c];
+                    }
+                } else {
+                    ov = ld(a.out + o);
+#pragma unroll
+                    for (int c = 0; c < C; ++c) {
+                        ov.re[c] += a.ckr * nx.re[c] - a.cki * nx.im[c];
+                        ov.im[c] += a.ckr * nx.im[c] + a.cki * nx.re[c];
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < C; ++c) bad |= !isfinite(ov.re[c]) || !isfinite(ov.im[c]);
+                st(a.out + o, ov);
+            }
+        }
+    }
+    if (MODE == MODE_SERIES) {
+        if (bad) atomicOr(a.status, 1);
+    }
+    if (MODE == MODE_DIRECT || MODE == MODE_DOUBLING) {
+        const int ncol = mp.U * C;
+        cta_column_sums<MU, C>(acc0, mp, ncol, smem, a.partial);
+        if (MODE == MODE_DOUBLING)
+            cta_column_sums<MU, C>(acc1, mp, ncol, smem, a.partial + (size_t)gridDim.x * ncol);
+        if (last_cta(a.ticket)) {
+            double2 *tot = smem;  // scratch of blockDim.x entries for the final combine
+            __shared__ double2 outbuf[512];  // ncol <= 8 units * 32 lanes * 2 columns
+            final_column_sums(a.partial, gridDim.x, ncol, tot, outbuf);
+            if (MODE == MODE_DIRECT) {
+                for (int j = threadIdx.x; j < a.bcols; j += blockDim.x)
+                    a.mu[(size_t)a.kmom * a.bcols + j] = outbuf[j].x;
+            } else {
+                __syncthreads();
+                // outbuf holds the even sums; stage them before computing odd sums
+                __shared__ double even[512];
+                for (int j = threadIdx.x; j < ncol; j += blockDim.x) even[j] = outbuf[j].x;
+                __syncthreads();
+                final_column_sums(a.partial + (size_t)gridDim.x * ncol, gridDim.x, ncol, tot, outbuf);
+                const int64_t nn = a.kmom;
+                for (int j = threadIdx.x; j < a.bcols; j += blockDim.x) {
+                    const double se = even[j], so = outbuf[j].x;
+                    if (nn == 0) {
+                        a.mu[j] = se;
+                        if (a.mlen > 1) a.mu[(size_t)a.bcols + j] = so;
+                    } else {
+                        const double mu0 = a.mu[j], mu1 = a.mu[(size_t)a.bcols + j];
+                        if (2 * nn < a.mlen) a.mu[(size_t)(2 * nn) * a.bcols + j] = 2. * se - mu0;
+                        if (2 * nn + 1 < a.mlen) a.mu[(size_t)(2 * nn + 1) * a.bcols + j] = 2. * so - mu1;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ sampling
+// One Clenshaw step of the metric sampler (Metric::sample, native.cpp:453-479):
+//   act = (z .* S (z .* b1) - center b1) / half
+//   FINAL = 0: b0 = 2 act - b2 + c xi   (written over b2)
+//   FINAL = 1: out = z .* (act - b2 + c xi)
+template <int FINAL>
+__global__ void __launch_bounds__(256) clenshaw_kernel(CsrView<double> S, const double *z, const double2 *b1,
+                                                       double2 *b2, const double2 *xi, double2 *out,
+                                                       double coef, double center, double half,
+                                                       int64_t n, RowMap mp) {
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < n; row += (int64_t)gridDim.x * mp.gpc) {
+        const int k0 = __ldg(S.ptr + row), k1 = __ldg(S.ptr + row + 1);
+        const double zr = __ldg(z + row);
+        for (int u = lane; u < mp.U; u += mp.G) {
+            double sr = 0., si = 0.;
+            for (int k = k0; k < k1; ++k) {
+                const int col = __ldg(S.idx + k);
+                const double zc = __ldg(z + col);
+                const double2 bv = __ldg(b1 + (size_t)col * mp.U + u);
+                const double xr = bv.x * zc, xi_ = bv.y * zc;
+                const double vr = __ldg(S.re + k), vi = S.im ? __ldg(S.im + k) : 0.;
+                sr += vr * xr - vi * xi_;
+                si += vr * xi_ + vi * xr;
+            }
+            const size_t o = (size_t)row * mp.U + u;
+            const double2 b = b1[o];
+            const double ar = (zr * sr - center * b.x) / half;
+            const double ai = (zr * si - center * b.y) / half;
+            const double2 p2 = b2[o];
+            const double2 x = xi[o];
+            if (FINAL == 0) {
+                b2[o] = make_double2(2. * ar - p2.x + coef * x.x, 2. * ai - p2.y + coef * x.y);
+            } else {
+                out[o] = make_double2(zr * (ar - p2.x + coef * x.x), zr * (ai - p2.y + coef * x.y));
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ conversions
+static __global__ void to_f32_kernel(const double2 *src, float4 *dst, int64_t n, int bsrc, int upad) {
+    // src: (n, bsrc) complex128; dst: (n, upad) float4 units (2 complex each),
+    // zero-padding columns >= bsrc.
+    const int64_t total = n * upad;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = i / upad;
+        const int u = (int)(i - row * upad);
+        const int j0 = 2 * u, j1 = 2 * u + 1;
+        const double2 a = j0 < bsrc ? src[row * bsrc + j0] : make_double2(0., 0.);
+        const double2 b = j1 < bsrc ? src[row * bsrc + j1] : make_double2(0., 0.);
+        dst[i] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
+    }
+}
+static __global__ void to_f64_kernel(const float4 *src, double2 *dst, int64_t n, int bdst, int upad) {
+    const int64_t total = n * (int64_t)bdst;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = i / bdst;
+        const int j = (int)(i - row * bdst);
+        const float4 v = src[row * upad + j / 2];
+        dst[i] = (j & 1) ? make_double2(v.z, v.w) : make_double2(v.x, v.y);
+    }
+}
+
+// Strided column-slice copy: dst(n, bd) = src(n, bs)[:, off:off+bd] (complex128).
+static __global__ void slice_kernel(const double2 *src, double2 *dst, int64_t n, int bs, int off, int bd) {
+    const int64_t total = n * (int64_t)bd;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = i / bd;
+        const int j = (int)(i - row * bd);
+        dst[i] = src[row * bs + off + j];
+    }
+}
+
+// y = sum_m coef_m * x_m over complex128 arrays of `len` elements (up to 4 terms;
+// y may alias one of the inputs only if it is read at the same index).
+struct Lincomb {
+    const double2 *x[4];
+    double cr[4], ci[4];
+    int terms;
+    int accumulate;  // y += ... instead of y = ...
+};
+static __global__ void lincomb_kernel(Lincomb L, double2 *y, int64_t len) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double sr = 0., si = 0.;
+        if (L.accumulate) {
+            const double2 v = y[i];
+            sr = v.x;
+            si = v.y;
+        }
+        for (int t = 0; t < L.terms; ++t) {
+            const double2 v = L.x[t][i];
+            sr += L.cr[t] * v.x - L.ci[t] * v.y;
+            si += L.cr[t] * v.y + L.ci[t] * v.x;
+        }
+        y[i] = make_double2(sr, si);
+    }
+}
+
+// Nonfinite scan: status |= 1 if any element is nonfinite.
+static __global__ void finite_scan_kernel(const double2 *x, int64_t len, int *status) {
+    bool bad = false;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 v = x[i];
+        bad |= !isfinite(v.x) || !isfinite(v.y);
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(status, 1);
+}
+
+}  // namespace kmsd

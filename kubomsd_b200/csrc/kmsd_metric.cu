@@ -1,0 +1,1056 @@
+// Overlap metric of the B200 engine: batched preconditioned CG for S^-1 and
+// the Chebyshev (Clenshaw) sampler for S^-1/2.
+//
+// The solve follows Metric::solve of the reference (cpp/native.cpp:313-452)
+// column by column: RHS scaling by safe_j = max_i max(|Re|,|Im|)
+// (native.cpp:320-329), thresholds max(rtol*||q_j||, atol/safe_j) (333),
+// curvature breakdown test (363-371), fixed / adaptive true-residual refresh
+// with restart (379-402), beta with the rz == 0 guard (405-408), final
+// true-residual acceptance (413-423) and representability checks (424-444).
+// All columns advance together; per-column scalars (alpha, beta, active, ...)
+// live on the device and are updated by the last CTA of each reduction
+// kernel, so an iteration needs no host round trip.  The host polls a single
+// halt word once per chunk of iterations to stop launching.
+#include <math.h>
+#include <float.h>
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <utility>
+
+#include "kmsd.h"
+#include "kmsd_impl.h"
+#include "kmsd_kernels.cuh"
+
+using namespace kmsd;
+
+namespace {
+
+struct ColPtr {
+    double *safe, *bn, *thr, *rz, *alpha, *beta, *rn, *tn, *newrz, *gap, *relative, *residual;
+    int *active, *restart, *brk, *conv, *finp, *fino;
+    long long *iters;
+    int *flags;  // [0] halt, [1] check, [2] nonfinite rhs, [3] breakdown, [4] n_active
+};
+constexpr int kDoubles = 12, kInts = 6;
+size_t col_bytes(int64_t b) { return (size_t)b * (kDoubles * 8 + kInts * 4 + 8) + 64; }
+ColPtr col_ptr(void *base, int64_t b) {
+    ColPtr c;
+    double *d = static_cast<double *>(base);
+    double **dp[kDoubles] = {&c.safe, &c.bn, &c.thr, &c.rz, &c.alpha, &c.beta,
+                             &c.rn, &c.tn, &c.newrz, &c.gap, &c.relative, &c.residual};
+    for (int i = 0; i < kDoubles; ++i) *dp[i] = d + (size_t)i * b;
+    long long *l = reinterpret_cast<long long *>(d + (size_t)kDoubles * b);
+    c.iters = l;
+    int *ip = reinterpret_cast<int *>(l + b);
+    int **ipp[kInts] = {&c.active, &c.restart, &c.brk, &c.conv, &c.finp, &c.fino};
+    for (int i = 0; i < kInts; ++i) *ipp[i] = ip + (size_t)i * b;
+    c.flags = ip + (size_t)kInts * b;
+    return c;
+}
+// device counters: [0] refreshes [1] checks [2] restarts [3] iterations sum; [4] max relative (double bits)
+struct Counters {
+    long long v[4];
+    double max_rel;
+};
+
+struct Pre {
+    const double *diag;
+    const int *bstart;
+    const int64_t *foff;
+    const double2 *factors;
+};
+
+__device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+    if (fabs(b.x) >= fabs(b.y)) {
+        const double r = b.y / b.x, den = b.x + b.y * r;
+        return make_double2((a.x + a.y * r) / den, (a.y - a.x * r) / den);
+    }
+    const double r = b.x / b.y, den = b.x * r + b.y;
+    return make_double2((a.x * r + a.y) / den, (a.y * r - a.x) / den);
+}
+
+// Rows of preconditioner block bi: [r0, r0+m).
+template <int MAXB>
+__device__ __forceinline__ void block_rows(const Pre &P, int64_t bi, int64_t &r0, int &m) {
+    if (MAXB == 1) {
+        r0 = bi;
+        m = 1;
+    } else {
+        r0 = P.bstart[bi];
+        m = P.bstart[bi + 1] - (int)r0;
+    }
+}
+
+// z = M^-1 r on one block for one column (native.cpp:259-277 diagonal and
+// block-Jacobi forward/back substitution with the lower Cholesky factor).
+template <int MAXB>
+__device__ __forceinline__ void precond(const Pre &P, int64_t bi, int64_t r0, int m, const double2 (&r)[MAXB],
+                                        double2 (&z)[MAXB]) {
+    if (MAXB == 1) {
+        const double d = P.diag[r0];
+        z[0] = make_double2(r[0].x / d, r[0].y / d);
+        return;
+    }
+    const double2 *L = P.factors + P.foff[bi];
+    if constexpr (MAXB > 8) {
+        // Large blocks: plain loops (registers spill to local memory).
+        for (int i = 0; i < m; ++i) {
+            double2 v = r[i];
+            for (int k = 0; k < i; ++k) {
+                const double2 l = L[i * m + k];
+                v.x -= l.x * z[k].x - l.y * z[k].y;
+                v.y -= l.x * z[k].y + l.y * z[k].x;
+            }
+            z[i] = cdiv(v, L[i * m + i]);
+        }
+        for (int i = m - 1; i >= 0; --i) {
+            double2 v = z[i];
+            for (int k = i + 1; k < m; ++k) {
+                const double2 l = L[k * m + i];
+                v.x -= l.x * z[k].x + l.y * z[k].y;
+                v.y -= l.x * z[k].y - l.y * z[k].x;
+            }
+            const double2 d = L[i * m + i];
+            z[i] = cdiv(v, make_double2(d.x, -d.y));
+        }
+        return;
+    }
+#pragma unroll
+    for (int i = 0; i < MAXB; ++i) {
+        if (i < m) {
+            double2 v = r[i];
+#pragma unroll
+            for (int k = 0; k < MAXB; ++k) {
+                if (k < i) {
+                    const double2 l = L[i * m + k];
+                    v.x -= l.x * z[k].x - l.y * z[k].y;
+                    v.y -= l.x * z[k].y + l.y * z[k].x;
+                }
+            }
+            z[i] = cdiv(v, L[i * m + i]);
+        }
+    }
+#pragma unroll
+    for (int i = MAXB - 1; i >= 0; --i) {
+        if (i < m) {
+            double2 v = z[i];
+#pragma unroll
+            for (int k = 0; k < MAXB; ++k) {
+                if (k > i && k < m) {
+                    const double2 l = L[k * m + i];  // conj(l) * z[k]
+                    v.x -= l.x * z[k].x + l.y * z[k].y;
+                    v.y -= l.x * z[k].y - l.y * z[k].x;
+                }
+            }
+            const double2 d = L[i * m + i];
+            z[i] = cdiv(v, make_double2(d.x, -d.y));
+        }
+    }
+}
+
+#define ZERO_ACC(acc)                                   \
+    _Pragma("unroll") for (int m_ = 0; m_ < MU; ++m_) { \
+        acc[m_][0] = make_double2(0., 0.);              \
+    }
+
+// ---- column scale: safe_j = max_i max(|Re|,|Im|), nonfinite detection
+template <int MU>
+__global__ void __launch_bounds__(256) pcg_scale_kernel(const double2 *B, int64_t n, RowMap mp, ColPtr c,
+                                                        double *partial, Ticket *tk) {
+    extern __shared__ double2 smem2[];
+    double *smem = reinterpret_cast<double *>(smem2);
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    double acc[MU][1];
+#pragma unroll
+    for (int m = 0; m < MU; ++m) acc[m][0] = 0.;
+    bool bad = false;
+    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < n; row += (int64_t)gridDim.x * mp.gpc) {
+#pragma unroll
+        for (int m = 0; m < MU; ++m) {
+            const int u = lane + m * mp.G;
+            if (u < mp.U) {
+                const double2 v = B[(size_t)row * mp.U + u];
+                bad |= !isfinite(v.x) || !isfinite(v.y);
+                acc[m][0] = fmax(acc[m][0], fmax(fabs(v.x), fabs(v.y)));
+            }
+        }
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(c.flags + 2, 1);
+    cta_column_max<MU, 1>(acc, mp, mp.U, smem, partial);
+    if (last_cta(tk)) {
+        final_column_max(partial, gridDim.x, mp.U, c.safe);
+        __syncthreads();
+        for (int j = threadIdx.x; j < mp.U; j += blockDim.x)
+            if (c.safe[j] == 0.) c.safe[j] = 1.;
+    }
+}
+
+// ---- init: q = B/safe, r = q, y = 0, z = M^-1 r; sums |q|^2 and Re<r,z>
+template <int MU, int MAXB>
+__global__ void __launch_bounds__(256) pcg_init_kernel(const double2 *B, double2 *q, double2 *y, double2 *r,
+                                                       double2 *z, Pre P, int64_t nb, RowMap mp, ColPtr c,
+                                                       double rtol, double atol, double2 *partial, Ticket *tk) {
+    extern __shared__ double2 smem[];
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    const int U = mp.U;
+    double2 acc[MU][1];
+    ZERO_ACC(acc);
+    for (int64_t bi = (int64_t)blockIdx.x * mp.gpc + g; bi < nb; bi += (int64_t)gridDim.x * mp.gpc) {
+        int64_t r0;
+        int m;
+        block_rows<MAXB>(P, bi, r0, m);
+#pragma unroll
+        for (int mm = 0; mm < MU; ++mm) {
+            const int u = lane + mm * mp.G;
+            if (u >= U) continue;
+            const double sf = c.safe[u];
+            double2 rr[MAXB], zz[MAXB];
+#pragma unroll
+            for (int i = 0; i < MAXB; ++i) {
+                if (i < m) {
+                    const size_t o = (size_t)(r0 + i) * U + u;
+                    const double2 v = B[o];
+                    const double2 qq = make_double2(v.x / sf, v.y / sf);
+                    q[o] = qq;
+                    r[o] = qq;
+                    y[o] = make_double2(0., 0.);
+                    rr[i] = qq;
+                    acc[mm][0].x += qq.x * qq.x + qq.y * qq.y;
+                }
+            }
+            precond<MAXB>(P, bi, r0, m, rr, zz);
+#pragma unroll
+            for (int i = 0; i < MAXB; ++i) {
+                if (i < m) {
+                    z[(size_t)(r0 + i) * U + u] = zz[i];
+                    acc[mm][0].y += rr[i].x * zz[i].x + rr[i].y * zz[i].y;
+                }
+            }
+        }
+    }
+    cta_column_sums<MU, 1>(acc, mp, U, smem, partial);
+    if (last_cta(tk)) {
+        __shared__ double2 tot[256];
+        final_column_sums(partial, gridDim.x, U, smem, tot);
+        __syncthreads();
+        const int j = threadIdx.x;
+        bool act = false;
+        if (j < U) {
+            const double bn = sqrt(tot[j].x);
+            const double thr = fmax(rtol * bn, atol / c.safe[j]);
+            act = bn > thr;
+            c.bn[j] = bn;
+            c.thr[j] = thr;
+            c.active[j] = act;
+            c.rz[j] = tot[j].y;
+            c.iters[j] = 0;
+            c.brk[j] = 0;
+            c.restart[j] = 0;
+            c.alpha[j] = 0.;
+            c.beta[j] = 0.;
+        }
+        const int nact = __syncthreads_count(act);
+        if (threadIdx.x == 0) {
+            c.flags[0] = nact == 0;  // halt: nothing to iterate
+            c.flags[1] = 0;
+            c.flags[3] = 0;
+            c.flags[4] = nact;
+        }
+    }
+}
+
+// p = active ? z : 0
+__global__ void pcg_pinit_kernel(const double2 *z, double2 *p, int64_t len, int U, ColPtr c) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int j = (int)(i % U);
+        p[i] = c.active[j] ? z[i] : make_double2(0., 0.);
+    }
+}
+
+// ---- sp = S p, curvature <p, sp>, alpha, breakdown
+template <int MU>
+__global__ void __launch_bounds__(256) pcg_spmv_kernel(CsrView<double> S, const double2 *p, double2 *sp,
+                                                       int64_t n, RowMap mp, ColPtr c, double2 *partial,
+                                                       Ticket *tk) {
+    if (*(volatile int *)c.flags) return;
+    extern __shared__ double2 smem[];
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    double2 acc[MU][1];
+    ZERO_ACC(acc);
+    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < n; row += (int64_t)gridDim.x * mp.gpc) {
+        Pk<double> yv[MU];
+#pragma unroll
+        for (int m = 0; m < MU; ++m) yv[m] = pk_zero<double>();
+        gather_row<double, MU>(S, p, row, mp.U, mp.G, lane, yv);
+#pragma unroll
+        for (int m = 0; m < MU; ++m) {
+            const int u = lane + m * mp.G;
+            if (u < mp.U) {
+                const size_t o = (size_t)row * mp.U + u;
+                sp[o] = make_double2(yv[m].re[0], yv[m].im[0]);
+                const double2 x = p[o];
+                acc[m][0].x += x.x * yv[m].re[0] + x.y * yv[m].im[0];
+                acc[m][0].y += x.x * yv[m].im[0] - x.y * yv[m].re[0];
+            }
+        }
+    }
+    cta_column_sums<MU, 1>(acc, mp, mp.U, smem, partial);
+    if (last_cta(tk)) {
+        __shared__ double2 tot[256];
+        final_column_sums(partial, gridDim.x, mp.U, smem, tot);
+        __syncthreads();
+        const int j = threadIdx.x;
+        bool b = false;
+        if (j < mp.U) {
+            const double cr = tot[j].x, ci = tot[j].y;
+            const bool act = c.active[j];
+            if (act && (!(cr > 0.) || !isfinite(cr) || !isfinite(ci) || fabs(ci) > 1e-10 * fmax(fabs(cr), DBL_MIN))) {
+                c.brk[j] = 1;
+                b = true;
+            }
+            c.alpha[j] = act ? c.rz[j] / cr : 0.;
+        }
+        if (__syncthreads_or(b) && threadIdx.x == 0) {
+            c.flags[3] = 1;
+            c.flags[0] = 1;
+        }
+    }
+}
+
+// ---- y += alpha p, r -= alpha sp, z = M^-1 r; sums |r|^2, Re<r,z>
+template <int MU, int MAXB>
+__global__ void __launch_bounds__(256) pcg_update_kernel(double2 *y, double2 *r, double2 *z, const double2 *p,
+                                                         const double2 *sp, Pre P, int64_t nb, RowMap mp, ColPtr c,
+                                                         int refresh, int adaptive, double2 *partial, Ticket *tk) {
+    if (*(volatile int *)c.flags) return;
+    extern __shared__ double2 smem[];
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    const int U = mp.U;
+    double2 acc[MU][1];
+    ZERO_ACC(acc);
+    for (int64_t bi = (int64_t)blockIdx.x * mp.gpc + g; bi < nb; bi += (int64_t)gridDim.x * mp.gpc) {
+        int64_t r0;
+        int m;
+        block_rows<MAXB>(P, bi, r0, m);
+#pragma unroll
+        for (int mm = 0; mm < MU; ++mm) {
+            const int u = lane + mm * mp.G;
+            if (u >= U) continue;
+            const double al = c.alpha[u];
+            double2 rr[MAXB], zz[MAXB];
+#pragma unroll
+            for (int i = 0; i < MAXB; ++i) {
+                if (i < m) {
+                    const size_t o = (size_t)(r0 + i) * U + u;
+                    const double2 pv = p[o], sv = sp[o];
+                    double2 yv = y[o], rv = r[o];
+                    yv.x += pv.x * al;
+                    yv.y += pv.y * al;
+                    rv.x -= sv.x * al;
+                    rv.y -= sv.y * al;
+                    y[o] = yv;
+                    r[o] = rv;
+                    rr[i] = rv;
+                    acc[mm][0].x += rv.x * rv.x + rv.y * rv.y;
+                }
+            }
+            precond<MAXB>(P, bi, r0, m, rr, zz);
+#pragma unroll
+            for (int i = 0; i < MAXB; ++i) {
+                if (i < m) {
+                    z[(size_t)(r0 + i) * U + u] = zz[i];
+                    acc[mm][0].y += rr[i].x * zz[i].x + rr[i].y * zz[i].y;
+                }
+            }
+        }
+    }
+    cta_column_sums<MU, 1>(acc, mp, U, smem, partial);
+    if (last_cta(tk)) {
+        __shared__ double2 tot[256];
+        final_column_sums(partial, gridDim.x, U, smem, tot);
+        __syncthreads();
+        const int j = threadIdx.x;
+        bool cand = false;
+        if (j < U) {
+            const int act = c.active[j];
+            c.iters[j] += act;
+            const double rn = sqrt(tot[j].x);
+            c.rn[j] = rn;
+            c.newrz[j] = tot[j].y;
+            cand = act && rn <= c.thr[j];
+        }
+        const bool candidate = __syncthreads_or(cand);
+        const bool check = refresh || (adaptive && candidate);
+        bool act_now = false;
+        if (j < U) {
+            if (!check) {
+                int act = c.active[j];
+                if (!adaptive) act = act && c.rn[j] > c.thr[j];
+                c.active[j] = act;
+                c.restart[j] = 0;
+                const double rz = c.rz[j], nrz = c.newrz[j];
+                c.beta[j] = act ? nrz / (rz != 0. ? rz : 1.) : 0.;
+                c.rz[j] = nrz;
+                act_now = act;
+            }
+        }
+        const int nact = __syncthreads_count(act_now);
+        if (threadIdx.x == 0) {
+            c.flags[1] = check;
+            if (!check) {
+                c.flags[4] = nact;
+                if (nact == 0) c.flags[0] = 1;
+            }
+        }
+    }
+}
+
+// ---- true residual t = q - S y; sums |t|^2 and |t - r|^2; refresh decision
+template <int MU>
+__global__ void __launch_bounds__(256) pcg_true_residual_kernel(CsrView<double> S, const double2 *q,
+                                                                const double2 *y, const double2 *r, double2 *t,
+                                                                int64_t n, RowMap mp, ColPtr c, int adaptive,
+                                                                double gap_ratio, double2 *partial, Ticket *tk,
+                                                                Counters *cnt) {
+    if (*(volatile int *)c.flags || !*(volatile int *)(c.flags + 1)) return;
+    extern __shared__ double2 smem[];
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    double2 acc[MU][1];
+    ZERO_ACC(acc);
+    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < n; row += (int64_t)gridDim.x * mp.gpc) {
+        Pk<double> sy[MU];
+#pragma unroll
+        for (int m = 0; m < MU; ++m) sy[m] = pk_zero<double>();
+        gather_row<double, MU>(S, y, row, mp.U, mp.G, lane, sy);
+#pragma unroll
+        for (int m = 0; m < MU; ++m) {
+            const int u = lane + m * mp.G;
+            if (u < mp.U) {
+                const size_t o = (size_t)row * mp.U + u;
+                const double2 qv = q[o], rv = r[o];
+                const double2 tv = make_double2(qv.x - sy[m].re[0], qv.y - sy[m].im[0]);
+                t[o] = tv;
+                acc[m][0].x += tv.x * tv.x + tv.y * tv.y;
+                const double dx = tv.x - rv.x, dy = tv.y - rv.y;
+                acc[m][0].y += dx * dx + dy * dy;
+            }
+        }
+    }
+    cta_column_sums<MU, 1>(acc, mp, mp.U, smem, partial);
+    if (last_cta(tk)) {
+        __shared__ double2 tot[256];
+        final_column_sums(partial, gridDim.x, mp.U, smem, tot);
+        __syncthreads();
+        const int j = threadIdx.x;
+        bool rs = false;
+        if (j < mp.U) {
+            int act = c.active[j];
+            int restart = 0;
+            if (act) {
+                const double tn = sqrt(tot[j].x), thr = c.thr[j];
+                if (adaptive) {
+                    const double gap = sqrt(tot[j].y);
+                    restart = tn > thr && (gap > gap_ratio * fmax(tn, thr) || c.rn[j] <= thr);
+                } else {
+                    restart = 1;
+                }
+                act = tn > thr;
+                c.tn[j] = tn;
+            }
+            c.active[j] = act;
+            c.restart[j] = restart;
+            rs = restart;
+        }
+        const int nrs = __syncthreads_count(rs);
+        if (threadIdx.x == 0) {
+            cnt->v[0] += 1;  // true_residual_refreshes
+            cnt->v[1] += 1;  // true_residual_checks
+            cnt->v[2] += nrs;
+        }
+    }
+}
+
+// ---- after a check: r <- t on restarted columns, z = M^-1 r, beta
+template <int MU, int MAXB>
+__global__ void __launch_bounds__(256) pcg_restart_kernel(double2 *r, double2 *z, const double2 *t, Pre P,
+                                                          int64_t nb, RowMap mp, ColPtr c, double2 *partial,
+                                                          Ticket *tk) {
+    if (*(volatile int *)c.flags || !*(volatile int *)(c.flags + 1)) return;
+    extern __shared__ double2 smem[];
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    const int U = mp.U;
+    double2 acc[MU][1];
+    ZERO_ACC(acc);
+    for (int64_t bi = (int64_t)blockIdx.x * mp.gpc + g; bi < nb; bi += (int64_t)gridDim.x * mp.gpc) {
+        int64_t r0;
+        int m;
+        block_rows<MAXB>(P, bi, r0, m);
+#pragma unroll
+        for (int mm = 0; mm < MU; ++mm) {
+            const int u = lane + mm * mp.G;
+            if (u >= U) continue;
+            const int rs = c.restart[u];
+            double2 rr[MAXB], zz[MAXB];
+#pragma unroll
+            for (int i = 0; i < MAXB; ++i) {
+                if (i < m) {
+                    const size_t o = (size_t)(r0 + i) * U + u;
+                    double2 rv = r[o];
+                    if (rs) {
+                        rv = t[o];
+                        r[o] = rv;
+                    }
+                    rr[i] = rv;
+                }
+            }
+            precond<MAXB>(P, bi, r0, m, rr, zz);
+#pragma unroll
+            for (int i = 0; i < MAXB; ++i) {
+                if (i < m) {
+                    z[(size_t)(r0 + i) * U + u] = zz[i];
+                    acc[mm][0].y += rr[i].x * zz[i].x + rr[i].y * zz[i].y;
+                }
+            }
+        }
+    }
+    cta_column_sums<MU, 1>(acc, mp, U, smem, partial);
+    if (last_cta(tk)) {
+        __shared__ double2 tot[256];
+        final_column_sums(partial, gridDim.x, U, smem, tot);
+        __syncthreads();
+        const int j = threadIdx.x;
+        bool act = false;
+        if (j < U) {
+            act = c.active[j];
+            const double rz = c.rz[j], nrz = tot[j].y;
+            c.beta[j] = act ? nrz / (rz != 0. ? rz : 1.) : 0.;
+            c.rz[j] = nrz;
+        }
+        const int nact = __syncthreads_count(act);
+        if (threadIdx.x == 0) {
+            c.flags[1] = 0;
+            c.flags[4] = nact;
+            if (nact == 0) c.flags[0] = 1;
+        }
+    }
+}
+
+// p = active ? z + (restart ? 0 : beta p) : 0
+__global__ void pcg_direction_kernel(const double2 *z, double2 *p, int64_t len, int U, ColPtr c) {
+    if (*(volatile int *)c.flags) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int j = (int)(i % U);
+        if (!c.active[j]) {
+            p[i] = make_double2(0., 0.);
+        } else {
+            const double2 zv = z[i];
+            if (c.restart[j]) {
+                p[i] = zv;
+            } else {
+                const double2 pv = p[i];
+                const double be = c.beta[j];
+                p[i] = make_double2(zv.x + pv.x * be, zv.y + pv.y * be);
+            }
+        }
+    }
+}
+
+// ---- final acceptance: t = q - S y; converged, relative, residual
+template <int MU>
+__global__ void __launch_bounds__(256) pcg_final_kernel(CsrView<double> S, const double2 *q, const double2 *y,
+                                                        int64_t n, RowMap mp, ColPtr c, double2 *partial,
+                                                        Ticket *tk, Counters *cnt) {
+    extern __shared__ double2 smem[];
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    double2 acc[MU][1];
+    ZERO_ACC(acc);
+    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < n; row += (int64_t)gridDim.x * mp.gpc) {
+        Pk<double> sy[MU];
+#pragma unroll
+        for (int m = 0; m < MU; ++m) sy[m] = pk_zero<double>();
+        gather_row<double, MU>(S, y, row, mp.U, mp.G, lane, sy);
+#pragma unroll
+        for (int m = 0; m < MU; ++m) {
+            const int u = lane + m * mp.G;
+            if (u < mp.U) {
+                const double2 qv = q[(size_t)row * mp.U + u];
+                const double tx = qv.x - sy[m].re[0], ty = qv.y - sy[m].im[0];
+                acc[m][0].x += tx * tx + ty * ty;
+            }
+        }
+    }
+    cta_column_sums<MU, 1>(acc, mp, mp.U, smem, partial);
+    if (last_cta(tk)) {
+        __shared__ double2 tot[256];
+        final_column_sums(partial, gridDim.x, mp.U, smem, tot);
+        __syncthreads();
+        const int j = threadIdx.x;
+        if (j < mp.U) {
+            const double rn = sqrt(tot[j].x), bn = c.bn[j];
+            c.conv[j] = rn <= c.thr[j] && !c.brk[j];
+            c.relative[j] = bn > 0. ? rn / bn : 0.;
+            c.residual[j] = rn * c.safe[j];
+            c.rn[j] = rn;
+        }
+        if (threadIdx.x == 0) cnt->v[1] += 1;
+    }
+}
+
+// ---- output: Y = y * safe with representability checks; status
+template <int MU>
+__global__ void __launch_bounds__(256) pcg_out_kernel(const double2 *y, double2 *Y, int64_t n, RowMap mp,
+                                                      ColPtr c, double2 *partial, Ticket *tk, Counters *cnt,
+                                                      int *status, FailReportFull *fr) {
+    extern __shared__ double2 smem[];
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    double2 acc[MU][1];
+    ZERO_ACC(acc);
+    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < n; row += (int64_t)gridDim.x * mp.gpc) {
+#pragma unroll
+        for (int m = 0; m < MU; ++m) {
+            const int u = lane + m * mp.G;
+            if (u < mp.U) {
+                const size_t o = (size_t)row * mp.U + u;
+                const double2 v = y[o];
+                const double sf = c.safe[u];
+                const double2 w = make_double2(v.x * sf, v.y * sf);
+                Y[o] = w;
+                acc[m][0].x += (!isfinite(v.x) || !isfinite(v.y)) ? 1. : 0.;
+                acc[m][0].y += (!isfinite(w.x) || !isfinite(w.y)) ? 1. : 0.;
+            }
+        }
+    }
+    cta_column_sums<MU, 1>(acc, mp, mp.U, smem, partial);
+    if (last_cta(tk)) {
+        __shared__ double2 tot[256];
+        final_column_sums(partial, gridDim.x, mp.U, smem, tot);
+        __syncthreads();
+        const int j = threadIdx.x;
+        bool notconv = false, unrep = false;
+        long long it = 0;
+        double rel = 0.;
+        if (j < mp.U) {
+            const int fin = tot[j].x == 0. && tot[j].y == 0.;
+            c.finp[j] = tot[j].x == 0.;
+            c.fino[j] = fin;
+            c.conv[j] = c.conv[j] && fin;
+            notconv = !c.conv[j];
+            unrep = !fin;
+            it = c.iters[j];
+            rel = c.relative[j];
+        }
+        const bool any_nc = __syncthreads_or(notconv);
+        const bool any_unrep = __syncthreads_or(unrep);
+        // max over columns of iterations and relative residual
+        __shared__ long long imax[256];
+        __shared__ double rmax[256];
+        imax[threadIdx.x] = it;
+        rmax[threadIdx.x] = rel;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            long long mi = 0;
+            double mr = cnt->max_rel;
+            for (int k = 0; k < (int)blockDim.x; ++k) {
+                mi = imax[k] > mi ? imax[k] : mi;
+                mr = fmax(mr, rmax[k]);
+            }
+            cnt->v[3] += mi;
+            cnt->max_rel = mr;
+            const bool nonfinite_rhs = c.flags[2] != 0;
+            const bool brk = c.flags[3] != 0;
+            if ((any_nc || brk || nonfinite_rhs) && status != nullptr && *status == 0) {
+                *status = nonfinite_rhs ? KMSD_EINVAL : KMSD_EMETRIC;
+                status[1] = 2;  // this solve owns the failure report
+                if (fr != nullptr) {
+                    fr->head.ncols = mp.U;
+                    fr->head.code = *status;
+                    fr->head.reason = nonfinite_rhs ? 3 : any_unrep ? 2 : brk ? 1 : 0;
+                }
+            }
+        }
+    }
+}
+
+// Copy the per-column report of a failed asynchronous solve (first failure).
+__global__ void pcg_copy_report_kernel(ColPtr c, int U, int *status, int *claimed, FailReportFull *fr) {
+    // Runs after pcg_out_kernel; only the solve that raised the status fills
+    // the report (claimed == 2), later ones leave it unchanged.
+    if (*claimed != 2) return;
+    __syncthreads();
+    for (int j = threadIdx.x; j < U && j < kMaxReportCols; j += blockDim.x) {
+        fr->converged[j] = (uint8_t)c.conv[j];
+        fr->breakdown[j] = (uint8_t)c.brk[j];
+        fr->iterations[j] = c.iters[j];
+        fr->true_residual[j] = c.residual[j];
+        fr->relative_residual[j] = c.relative[j];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *claimed = 1;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host side
+int kmsd_metric_s::ensure(int64_t b) {
+    if (b <= wb && q.p) return KMSD_OK;
+    const size_t bytes = (size_t)n * b * sizeof(double2);
+    for (DevBuf *d : {&q, &y, &r, &z, &p, &sp, &t})
+        if (d->ensure(bytes)) return KMSD_ECUDA;
+    if (cols.ensure(col_bytes(b))) return KMSD_ECUDA;
+    if (!dcount.p) {
+        if (dcount.ensure(sizeof(Counters))) return KMSD_ECUDA;
+        KMSD_CUDA(cudaMemset(dcount.p, 0, sizeof(Counters)));
+    }
+    if (!host_pinned.p) {
+        void *h = nullptr;
+        KMSD_CUDA(cudaMallocHost(&h, 64));
+        host_pinned.p = h;
+        host_pinned.bytes = 64;
+        KMSD_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+        KMSD_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+    }
+    wb = b;
+    return KMSD_OK;
+}
+
+namespace {
+
+template <int MU, int MAXB>
+int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rtol, double atol, int maxiter,
+            cudaStream_t s, int *status, FailReportFull *fr, int *claimed) {
+    const int64_t n = M->n;
+    const RowMap mp = make_map((int)b, kThreads);
+    const int64_t nb = MAXB == 1 ? n : M->nblocks;
+    const int grid_r = grid_for(n, mp), grid_b = grid_for(nb, mp);
+    const int grid_mx = grid_r > grid_b ? grid_r : grid_b;
+    if (M->red.ensure(grid_mx, (int)b)) return KMSD_ECUDA;
+    const size_t sm = reduce_smem(mp, 1);
+    ColPtr c = col_ptr(M->cols.p, b);
+    Pre P{M->diag, M->bstart, M->foff, M->factors};
+    const CsrView<double> S = M->S->view64();
+    Counters *cnt = M->dcount.as<Counters>();
+    double2 *q = M->q.as<double2>(), *y = M->y.as<double2>(), *r = M->r.as<double2>(), *z = M->z.as<double2>(),
+            *p = M->p.as<double2>(), *sp = M->sp.as<double2>(), *t = M->t.as<double2>();
+    double2 *part = M->red.part();
+    Ticket *tk = M->red.tick();
+    const int64_t len = n * b;
+    const int egrid = (int)std::min<int64_t>((len + 255) / 256, (int64_t)sm_count() * 16);
+
+    KMSD_CUDA(cudaMemsetAsync(c.flags, 0, 8 * sizeof(int), s));
+    pcg_scale_kernel<MU><<<grid_r, kThreads, sm, s>>>(B, n, mp, c, reinterpret_cast<double *>(part), tk);
+    count_launch();
+    pcg_init_kernel<MU, MAXB><<<grid_b, kThreads, sm, s>>>(B, q, y, r, z, P, nb, mp, c, rtol, atol, part, tk);
+    count_launch();
+    pcg_pinit_kernel<<<egrid, 256, 0, s>>>(z, p, len, (int)b, c);
+    count_launch();
+    volatile int *hflag = static_cast<volatile int *>(M->host_pinned.p);
+    const int chunk = 4;
+    int slot = 0, pending = 0;
+    for (int k = 0; k < maxiter; ++k) {
+        const int refresh = ((k + 1) % M->interval) == 0;
+        pcg_spmv_kernel<MU><<<grid_r, kThreads, sm, s>>>(S, p, sp, n, mp, c, part, tk);
+        count_launch();
+        pcg_update_kernel<MU, MAXB><<<grid_b, kThreads, sm, s>>>(y, r, z, p, sp, P, nb, mp, c, refresh,
+                                                                 M->adaptive, part, tk);
+        count_launch();
+        if (refresh || M->adaptive) {
+            pcg_true_residual_kernel<MU><<<grid_r, kThreads, sm, s>>>(S, q, y, r, t, n, mp, c, M->adaptive,
+                                                                     M->gap_ratio, part, tk, cnt);
+            count_launch();
+            pcg_restart_kernel<MU, MAXB><<<grid_b, kThreads, sm, s>>>(r, z, t, P, nb, mp, c, part, tk);
+            count_launch();
+        }
+        pcg_direction_kernel<<<egrid, 256, 0, s>>>(z, p, len, (int)b, c);
+        count_launch();
+        if ((k + 1) % chunk == 0) {
+            KMSD_CUDA(cudaMemcpyAsync((void *)(hflag + slot), c.flags, sizeof(int), cudaMemcpyDeviceToHost, s));
+            KMSD_CUDA(cudaEventRecord(M->ev[slot], s));
+            ++pending;
+            const int other = slot ^ 1;
+            if (pending >= 2) {
+                KMSD_CUDA(cudaEventSynchronize(M->ev[other]));
+                if (hflag[other]) break;
+            }
+            slot = other;
+        }
+    }
+    KMSD_CUDA(cudaGetLastError());
+    pcg_final_kernel<MU><<<grid_r, kThreads, sm, s>>>(S, q, y, n, mp, c, part, tk, cnt);
+    count_launch();
+    pcg_out_kernel<MU><<<grid_r, kThreads, sm, s>>>(y, Y, n, mp, c, part, tk, cnt, status, fr);
+    count_launch();
+    if (status != nullptr && fr != nullptr) {
+        pcg_copy_report_kernel<<<1, 256, 0, s>>>(c, (int)b, status, claimed, fr);
+        count_launch();
+    }
+    KMSD_CUDA(cudaGetLastError());
+    return KMSD_OK;
+}
+
+using PcgFn = int (*)(kmsd_metric_s *, const double2 *, double2 *, int64_t, double, double, int, cudaStream_t,
+                      int *, FailReportFull *, int *);
+
+template <int MAXB>
+PcgFn pick_mu(int mu) {
+    switch (mu) {
+        case 1: return run_pcg<1, MAXB>;
+        case 2: return run_pcg<2, MAXB>;
+        case 4: return run_pcg<4, MAXB>;
+        case 8: return run_pcg<8, MAXB>;
+    }
+    return nullptr;
+}
+PcgFn pick(int mu, int maxb) {
+    if (maxb <= 1) return pick_mu<1>(mu);
+    if (maxb <= 4) return pick_mu<4>(mu);
+    if (maxb <= 8) return pick_mu<8>(mu);
+    if (maxb <= 32) return pick_mu<32>(mu);
+    return nullptr;
+}
+
+}  // namespace
+
+int kmsd_metric_s::solve(const double2 *B, double2 *Y, int64_t b, double rtol, double atol, int maxiter,
+                         kmsd_solve_report *report, cudaStream_t s, int *status, void *fail_report) {
+    if (b < 1 || !std::isfinite(rtol) || !std::isfinite(atol) || rtol < 0 || atol < 0 || maxiter < 1)
+        return fail(KMSD_EINVAL, "invalid metric RHS shape/tolerances");
+    if (b > 256) return fail(KMSD_EINVAL, "metric solve supports at most 256 columns per call");
+    const auto start = std::chrono::steady_clock::now();
+    if (ensure(b)) return KMSD_ECUDA;
+    const RowMap mp = make_map((int)b, kThreads);
+    PcgFn fn = pick(mu_for(mp), nblocks ? maxb : 1);
+    if (!fn) return fail(KMSD_EINVAL, "unsupported metric block size / column count");
+    const bool sync = status == nullptr;
+    // Synchronous calls use a private status word and report.
+    static thread_local DevBuf own_status, own_report;
+    int *st = status;
+    FailReportFull *fr = static_cast<FailReportFull *>(fail_report);
+    int *claimed = nullptr;
+    if (sync) {
+        if (own_status.ensure(2 * sizeof(int))) return KMSD_ECUDA;
+        if (own_report.ensure(sizeof(FailReportFull))) return KMSD_ECUDA;
+        st = own_status.as<int>();
+        fr = own_report.as<FailReportFull>();
+        KMSD_CUDA(cudaMemsetAsync(st, 0, 2 * sizeof(int), s));
+    }
+    claimed = st + 1;
+    int rc = fn(this, B, Y, b, rtol, atol, maxiter, s, st, fr, claimed);
+    if (rc) return rc;
+    ++calls;
+    if (!sync) return KMSD_OK;
+    // Read status + per-column report.
+    ColPtr c = col_ptr(cols.p, b);
+    std::vector<int> conv(b), brk(b), flags(8);
+    std::vector<long long> it(b);
+    std::vector<double> res(b), rel(b);
+    int hst[2];
+    KMSD_CUDA(cudaMemcpyAsync(conv.data(), c.conv, b * sizeof(int), cudaMemcpyDeviceToHost, s));
+    KMSD_CUDA(cudaMemcpyAsync(brk.data(), c.brk, b * sizeof(int), cudaMemcpyDeviceToHost, s));
+    KMSD_CUDA(cudaMemcpyAsync(it.data(), c.iters, b * sizeof(long long), cudaMemcpyDeviceToHost, s));
+    KMSD_CUDA(cudaMemcpyAsync(res.data(), c.residual, b * sizeof(double), cudaMemcpyDeviceToHost, s));
+    KMSD_CUDA(cudaMemcpyAsync(rel.data(), c.relative, b * sizeof(double), cudaMemcpyDeviceToHost, s));
+    KMSD_CUDA(cudaMemcpyAsync(flags.data(), c.flags, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    KMSD_CUDA(cudaMemcpyAsync(hst, st, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    KMSD_CUDA(cudaStreamSynchronize(s));
+    seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+    if (report) {
+        for (int64_t j = 0; j < b; ++j) {
+            report->converged[j] = (uint8_t)conv[j];
+            report->breakdown[j] = (uint8_t)brk[j];
+            report->iterations[j] = it[j];
+            report->true_residual[j] = res[j];
+            report->relative_residual[j] = rel[j];
+        }
+    }
+    if (flags[2]) return fail(KMSD_EINVAL, "metric RHS must be finite");
+    if (hst[0]) {
+        // Reproduce the reference's message precedence (native.cpp:447-450).
+        std::vector<int> finp(b), fino(b);
+        KMSD_CUDA(cudaMemcpy(fino.data(), c.fino, b * sizeof(int), cudaMemcpyDeviceToHost));
+        bool representable = true;
+        for (int64_t j = 0; j < b; ++j) representable = representable && fino[j];
+        if (!representable)
+            return fail(KMSD_EMETRIC,
+                        "S solve solution is nonfinite or not representable in complex128 after rescaling");
+        if (flags[3]) return fail(KMSD_EMETRIC, "PCG non-positive/complex curvature breakdown");
+        return fail(KMSD_EMETRIC, "S solve failed true-residual acceptance");
+    }
+    return KMSD_OK;
+}
+
+// ------------------------------------------------------------------ sampling
+namespace {
+int sample_impl(kmsd_metric_s *M, const double2 *xi, double2 *out, int64_t b, const double *coeff,
+                int64_t ncoeff, double center, double half, cudaStream_t s) {
+    const int64_t n = M->n;
+    if (M->ensure(b)) return KMSD_ECUDA;
+    const RowMap mp = make_map((int)b, kThreads);
+    const int grid = grid_for(n, mp);
+    double2 *b1 = M->q.as<double2>(), *b2 = M->r.as<double2>();
+    const size_t bytes = (size_t)n * b * sizeof(double2);
+    const CsrView<double> S = M->S->view64();
+    if (ncoeff == 1) {
+        // out = z .* (0 + c0 xi)
+        KMSD_CUDA(cudaMemsetAsync(b1, 0, bytes, s));
+        KMSD_CUDA(cudaMemsetAsync(b2, 0, bytes, s));
+        // act(b1 = 0) = 0, so FINAL gives z .* (0 - 0 + c0 xi)
+        clenshaw_kernel<1><<<grid, kThreads, 0, s>>>(S, M->zinv, b1, b2, xi, out, coeff[0], center, 1.0, n, mp);
+        count_launch();
+        KMSD_CUDA(cudaGetLastError());
+        return KMSD_OK;
+    }
+    KMSD_CUDA(cudaMemsetAsync(b1, 0, bytes, s));
+    KMSD_CUDA(cudaMemsetAsync(b2, 0, bytes, s));
+    for (int64_t k = ncoeff - 1; k > 0; --k) {
+        // b0 = 2 act(b1) - b2 + c_k xi, written over b2; then swap roles.
+        clenshaw_kernel<0><<<grid, kThreads, 0, s>>>(S, M->zinv, b1, b2, xi, nullptr, coeff[k], center, half, n,
+                                                    mp);
+        count_launch();
+        std::swap(b1, b2);
+    }
+    clenshaw_kernel<1><<<grid, kThreads, 0, s>>>(S, M->zinv, b1, b2, xi, out, coeff[0], center, half, n, mp);
+    count_launch();
+    KMSD_CUDA(cudaGetLastError());
+    return KMSD_OK;
+}
+}  // namespace
+
+// ------------------------------------------------------------------ ABI
+extern "C" {
+
+int kmsd_metric_create(kmsd_csr s, const double *diag, int64_t nblocks, const int64_t *block_start,
+                       const int64_t *factor_offset, const double *factor_re, const double *factor_im,
+                       kmsd_metric *out) {
+    if (!s || !diag || !out) return fail(KMSD_EINVAL, "invalid metric diagonal/threads");
+    const int64_t n = s->n;
+    for (int64_t i = 0; i < n; ++i)
+        if (!(diag[i] > 0) || !std::isfinite(diag[i])) return fail(KMSD_EINVAL, "invalid metric diagonal");
+    int maxb = 1;
+    std::vector<int> bs;
+    std::vector<double2> fac;
+    std::vector<int64_t> offs;
+    if (nblocks > 0) {
+        if (!block_start || !factor_offset || !factor_re)
+            return fail(KMSD_EINVAL, "invalid block-Jacobi factor partition");
+        if (block_start[0] != 0) return fail(KMSD_EINVAL, "invalid block-Jacobi factor partition");
+        int64_t total = 0;
+        for (int64_t i = 0; i < nblocks; ++i) {
+            const int64_t a = block_start[i], bnd = block_start[i + 1];
+            if (bnd <= a || bnd > n) return fail(KMSD_EINVAL, "invalid block-Jacobi factor partition");
+            const int64_t m = bnd - a;
+            if (m > 32) return fail(KMSD_EINVAL, "block-Jacobi blocks larger than 32 rows are not supported");
+            if (m > maxb) maxb = (int)m;
+            total = std::max(total, factor_offset[i] + m * m);
+        }
+        if (block_start[nblocks] != n) return fail(KMSD_EINVAL, "incomplete block-Jacobi partition");
+        if (n > INT32_MAX) return fail(KMSD_EINVAL, "metric too large");
+        bs.assign(block_start, block_start + nblocks + 1);
+        offs.assign(factor_offset, factor_offset + nblocks);
+        fac.resize(total);
+        for (int64_t i = 0; i < total; ++i)
+            fac[i] = make_double2(factor_re[i], factor_im ? factor_im[i] : 0.);
+        for (int64_t i = 0; i < nblocks; ++i) {
+            const int64_t m = block_start[i + 1] - block_start[i];
+            for (int64_t d = 0; d < m; ++d) {
+                const double2 v = fac[offs[i] + d * m + d];
+                if (!(v.x != 0 || v.y != 0) || !std::isfinite(v.x) || !std::isfinite(v.y))
+                    return fail(KMSD_EINVAL, "invalid block-Jacobi factor partition");
+            }
+        }
+    }
+    auto *M = new kmsd_metric_s();
+    M->S = s;
+    M->n = n;
+    M->nblocks = nblocks;
+    M->maxb = maxb;
+    std::vector<double> zinv(n);
+    for (int64_t i = 0; i < n; ++i) zinv[i] = 1. / std::sqrt(diag[i]);
+    bool unit_diag = true;
+    for (int64_t i = 0; i < n; ++i) unit_diag = unit_diag && diag[i] == 1.;
+    M->identity = s->identity && nblocks == 0 && unit_diag;
+    auto up = [&](void **dst, const void *src, size_t bytes) -> int {
+        KMSD_CUDA(cudaMalloc(dst, bytes));
+        KMSD_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+        return KMSD_OK;
+    };
+    int rc = up((void **)&M->diag, diag, n * sizeof(double));
+    if (!rc) rc = up((void **)&M->zinv, zinv.data(), n * sizeof(double));
+    if (!rc && nblocks > 0) {
+        rc = up((void **)&M->bstart, bs.data(), bs.size() * sizeof(int));
+        if (!rc) rc = up((void **)&M->foff, offs.data(), offs.size() * sizeof(int64_t));
+        if (!rc) rc = up((void **)&M->factors, fac.data(), fac.size() * sizeof(double2));
+    }
+    if (rc) {
+        kmsd_metric_destroy(M);
+        return rc;
+    }
+    *out = M;
+    return KMSD_OK;
+}
+
+void kmsd_metric_destroy(kmsd_metric m) {
+    if (!m) return;
+    cudaFree(m->diag);
+    cudaFree(m->zinv);
+    cudaFree(m->bstart);
+    cudaFree(m->foff);
+    cudaFree(m->factors);
+    for (DevBuf *d : {&m->q, &m->y, &m->r, &m->z, &m->p, &m->sp, &m->t, &m->cols, &m->dcount}) d->release();
+    m->red.partial.release();
+    m->red.ticket.release();
+    if (m->host_pinned.p) cudaFreeHost(m->host_pinned.p);
+    for (auto &e : m->ev)
+        if (e) cudaEventDestroy(e);
+    delete m;
+}
+
+int kmsd_metric_set_residual_policy(kmsd_metric m, int policy, int interval, double gap_ratio) {
+    if (!m || (policy != 0 && policy != 1) || interval < 1 || !(gap_ratio > 0 && gap_ratio < 1))
+        return fail(KMSD_EINVAL, "invalid residual policy");
+    m->adaptive = policy;
+    m->interval = interval;
+    m->gap_ratio = gap_ratio;
+    return KMSD_OK;
+}
+
+int kmsd_metric_solve(kmsd_metric m, const void *b_in, void *y_out, int64_t b, double rtol, double atol,
+                      int maxiter, kmsd_solve_report *report, void *stream) {
+    if (!m || !b_in || !y_out) return fail(KMSD_EINVAL, "invalid metric RHS shape/tolerances");
+    return m->solve(static_cast<const double2 *>(b_in), static_cast<double2 *>(y_out), b, rtol, atol, maxiter,
+                    report, static_cast<cudaStream_t>(stream));
+}
+
+int kmsd_metric_sample(kmsd_metric m, const void *xi, void *out, int64_t b, const double *coeff, int64_t ncoeff,
+                       double center, double half, void *stream) {
+    if (!m || !xi || !out || b < 1 || ncoeff < 1 || !coeff) return fail(KMSD_EINVAL, "invalid sampling dimensions");
+    if (b > 256) return fail(KMSD_EINVAL, "sampling supports at most 256 columns per call");
+    if (ncoeff > 1 && !(half > 0)) return fail(KMSD_EINVAL, "sampling half-width must be positive");
+    return sample_impl(m, static_cast<const double2 *>(xi), static_cast<double2 *>(out), b, coeff, ncoeff, center,
+                       half, static_cast<cudaStream_t>(stream));
+}
+
+int kmsd_metric_stats_get(kmsd_metric m, kmsd_metric_stats *out) {
+    if (!m || !out) return fail(KMSD_EINVAL, "invalid metric");
+    Counters c{};
+    if (m->dcount.p) {
+        KMSD_CUDA(cudaDeviceSynchronize());
+        KMSD_CUDA(cudaMemcpy(&c, m->dcount.p, sizeof(Counters), cudaMemcpyDeviceToHost));
+    }
+    out->calls = m->calls;
+    out->max_iterations_sum = c.v[3];
+    out->seconds = m->seconds;
+    out->max_relative_residual = c.max_rel;
+    out->true_residual_refreshes = c.v[0];
+    out->true_residual_checks = c.v[1];
+    out->residual_restarts = c.v[2];
+    out->refinement_steps = 0;
+    return KMSD_OK;
+}
+
+int kmsd_metric_is_identity(kmsd_metric m) { return m && m->identity ? 1 : 0; }
+
+}  // extern "C"

@@ -1,0 +1,289 @@
+"""Generate the golden fixtures of tests/golden/ by running the REFERENCE.
+
+Runs KuboMSD's own Python solver layer (src/kubo_msd: build_operators,
+stepwise_samples, iter_stochastic_blocks, ...) on top of its compiled CPU
+engine cpp/native.cpp, built into oracle/_ref/ by oracle/build_ref.sh, with
+`cpu_kernel="cpp"` — the reference's production CPU path.  The outputs are
+stored as small .npz files together with their inputs; tests compare the B200
+engine and the oracle restatement against them.  Needs the reference checkout
+(default /root/reference, or $KUBOMSD_REFERENCE); h5py is not needed because
+only the solver layer is driven.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+from dataclasses import replace
+from pathlib import Path
+
+import numpy as np
+import scipy.linalg as la
+import scipy.sparse as sp
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+REF = Path(os.environ.get("KUBOMSD_REFERENCE", "/root/reference"))
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(REF / "src"))
+sys.path.insert(0, str(REF))
+
+from oracle import ref_native  # noqa: E402
+
+ref_native.build()
+import kubo_msd  # noqa: E402
+
+kubo_msd.__path__.append(str(ref_native.REF_DIR))  # kubo_msd._native from oracle/_ref
+
+from kubo_msd.config import RunConfig  # noqa: E402
+from kubo_msd.contracts import ModelBundle  # noqa: E402
+from kubo_msd.metric.sampling import MetricSampler, random_phases  # noqa: E402
+from kubo_msd.metric.solve import MetricSolver  # noqa: E402
+from kubo_msd.operators.velocity import build_operators  # noqa: E402
+from kubo_msd.solvers.chebyshev import bessel_coefficients, scaling  # noqa: E402
+from kubo_msd.solvers.stepwise import propagate, stepwise_samples  # noqa: E402
+from kubo_msd.solvers.stochastic import iter_stochastic_blocks  # noqa: E402
+from kubo_msd.kernels.energy import jackson_coefficients, reconstruction_matrix  # noqa: E402
+
+from kubomsd_b200 import lattices  # noqa: E402
+
+
+def csr_arrays(prefix, A):
+    A = sp.csr_matrix(A, dtype=np.complex128)
+    A.sum_duplicates()
+    A.sort_indices()
+    return {f"{prefix}_indptr": A.indptr.astype(np.int64), f"{prefix}_indices": A.indices.astype(np.int64),
+            f"{prefix}_data": A.data, f"{prefix}_shape": np.array(A.shape)}
+
+
+def digest(A):
+    A = sp.csr_matrix(A, dtype=np.complex128)
+    A.sum_duplicates()
+    A.sort_indices()
+    h = hashlib.sha256()
+    for v in (A.indptr.astype(np.int64), A.indices.astype(np.int64), A.data):
+        h.update(np.ascontiguousarray(v).tobytes())
+    return h.hexdigest()
+
+
+def small_model(kind, n=10, seed=7331):
+    """Dense complex Hermitian H, SPD S = I + 0.03 A^H A, position/velocity X."""
+    rng = np.random.default_rng(seed)
+    A = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    S = np.eye(n) + .03 * (A.conj().T @ A)
+    H = (A + A.conj().T) / 10
+    X = np.diag(np.linspace(-.6, .9, n)).astype(complex) + .02 * (A + A.conj().T)
+    if kind == "velocity":
+        return ModelBundle(H, S, velocity={"x": X}, atom_slices=[(0, 3), (3, 6), (6, 10)])
+    if kind == "position":
+        return ModelBundle(H, S, position={"x": X}, atom_slices=[(0, 3), (3, 6), (6, 10)])
+    r = np.linspace(0, 2.5, n)
+    comp = (H * (r[None, :] - r[:, None]), X - r[:, None] * S, X - S * r[None, :])
+    return ModelBundle(H, S, composite={"x": comp}, atom_slices=[(0, 3), (3, 6), (6, 10)])
+
+
+def base_config(**kw):
+    values = dict(energy_eV=[-.4, -.1, .2, .5], time_fs=[0, .08, .2], solver="stochastic-kpm",
+                  kernel="jackson", axes=("x",), spectral_bounds=(-2.5, 2.5), n_moments=24, metric_rtol=2e-13,
+                  sampling_tol=1e-12, segment_fs=.07, include_vac=False, cpu_kernel="cpp",
+                  stochastic_method="stepwise")
+    values.update(kw)
+    return RunConfig(**values)
+
+
+def engine_case(kind, precond):
+    m = small_model(kind)
+    cfg = base_config(preconditioner=precond)
+    ops = build_operators(m, cfg)
+    assert ops.native is not None and ops.metric.native is not None
+    rng = np.random.default_rng(4242)
+    n = m.n_orbitals
+    B = rng.normal(size=(n, 3)) + 1j * rng.normal(size=(n, 3))
+    c, a = scaling(cfg)
+    coeff, _ = bessel_coefficients(.07, cfg, weighted_tail=True)
+    aug = np.concatenate([B, rng.normal(size=(n, 3)) + 1j * rng.normal(size=(n, 3))], axis=1)
+    out = dict(B=B, aug=aug, coeff=coeff, center=c, half=a, rtol=cfg.metric_rtol,
+               H=np.asarray(m.H_cov), S=np.asarray(m.S),
+               blocks_L=np.array([np.pad(L, ((0, 4 - L.shape[0]), (0, 4 - L.shape[0])))
+                                  for _, _, L in ops.metric.host_setup.blocks]) if precond == "block-jacobi"
+               else np.zeros((0, 4, 4)),
+               blocks_start=np.array([0] + [b for _, b, _ in ops.metric.host_setup.blocks]) if precond ==
+               "block-jacobi" else np.zeros(0, np.int64))
+    if kind == "velocity":
+        out["V"] = np.asarray(m.velocity["x"])
+    elif kind == "position":
+        out["X"] = np.asarray(m.position["x"])
+    else:
+        out["bond"], out["xbar"], out["delta"] = (np.asarray(x) for x in m.composite["x"])
+    out["h_action"] = ops.native.h_action(B)
+    out["v_cov"] = ops.native.v_cov([1., 0., 0.], B)
+    out["chain"] = ops.native.chain(B, 12, c, a)
+    out["moments"] = ops.native.moments(B, 20, c, a)
+    out["series_plain"] = ops.native.series(B, coeff, c, a)
+    out["series_aug"] = ops.native.series(aug, coeff, c, a, [[1., 0., 0.]])
+    y, rep = ops.metric.solve_s(B)
+    out["solve"] = y
+    out["solve_iterations"] = np.asarray(rep.iterations)
+    out["solve_relative"] = np.asarray(rep.relative_residual)
+    sampler = MetricSampler(ops.metric, cfg)
+    xi = random_phases(n, 11, [0, 1, 2])
+    out["xi"] = xi
+    out["sample_coeff"] = np.asarray(sampler.coeff)
+    out["sample_center"] = sampler.center
+    out["sample_half"] = sampler.half
+    out["sample"] = sampler.transform(xi)
+    out["propagate"] = propagate(B, .2, ops, cfg)[0]
+    dos, nums, _ = stepwise_samples(ops, cfg, B)
+    out["dos"] = dos
+    out["msd"] = nums["msd_A2/commutator"]
+    out["energies"] = np.asarray(cfg.energy_eV)
+    out["times"] = np.asarray(cfg.time_fs)
+    out["n_moments"] = cfg.n_moments
+    out["segment_fs"] = cfg.segment_fs
+    out["bounds"] = np.asarray(cfg.spectral_bounds)
+    return out
+
+
+def pcg_known():
+    out = {}
+    cfg = base_config()
+    from types import SimpleNamespace
+    solver = MetricSolver(np.array([[1., .2], [.2, 2.]]), cfg)
+    y, rep = solver.solve_s(np.ones((2, 1)), SimpleNamespace(rtol=.5, metric_atol=0., metric_maxiter=1))
+    out["one_step"] = y
+    out["one_step_iterations"] = np.asarray(rep.iterations)
+    solver = MetricSolver(np.array([[1, .2j], [-.2j, 2]]), base_config(metric_maxiter=1))
+    try:
+        solver.solve_s(np.array([[0, 1], [0, 1]], complex))
+    except ValueError as exc:
+        d = exc.diagnostics
+        out["fail_converged"] = np.array(d["converged"])
+        out["fail_iterations"] = np.array(d["iterations"])
+        out["fail_message"] = np.array(str(exc))
+    rng = np.random.default_rng(97)
+    A = rng.normal(size=(11, 11)) + 1j * rng.normal(size=(11, 11))
+    S = A.conj().T @ A + 2 * np.eye(11)
+    B = rng.normal(size=(11, 4)) + 1j * rng.normal(size=(11, 4))
+    B *= [0, 1e-180, 1, 1e180]
+    out["scaled_S"] = S
+    out["scaled_B"] = B
+    for pre in ("diagonal", "block-jacobi"):
+        s = MetricSolver(S, base_config(preconditioner=pre), atom_slices=[(0, 3), (3, 7), (7, 11)])
+        y, rep = s.solve_s(B)
+        out[f"scaled_{pre}"] = y
+        out[f"scaled_{pre}_iterations"] = np.asarray(rep.iterations)
+    # a tridiagonal metric long enough to exercise the 32-iteration refresh
+    n = 96
+    T = sp.diags([-np.ones(n - 1), 2.03 * np.ones(n), -np.ones(n - 1)], [-1, 0, 1], format="csr", dtype=complex)
+    Bt = (rng.normal(size=(n, 3)) + 1j * rng.normal(size=(n, 3)))
+    s = MetricSolver(T, base_config(metric_rtol=1e-11, metric_maxiter=1000))
+    y, rep = s.solve_s(Bt)
+    out["tri_B"] = Bt
+    out["tri"] = y
+    out["tri_iterations"] = np.asarray(rep.iterations)
+    out["tri_refreshes"] = s.diagnostics()["true_residual_refreshes"]
+    for pol in ("adaptive",):
+        s = MetricSolver(T, base_config(metric_rtol=1e-11, metric_maxiter=1000, metric_residual_policy=pol))
+        y, rep = s.solve_s(Bt)
+        out[f"tri_{pol}"] = y
+        out[f"tri_{pol}_iterations"] = np.asarray(rep.iterations)
+    return out
+
+
+def host_formulas():
+    out = {}
+    cfg = base_config(spectral_bounds=(-11.2, 11.2))
+    for tag, dt, w in (("a", 1., True), ("b", .3, False), ("c", .07, True)):
+        b, d = bessel_coefficients(dt, cfg, weighted_tail=w)
+        out[f"bessel_{tag}"] = b
+    for L in (1, 2, 64, 1024):
+        out[f"jackson_{L}"] = jackson_coefficients(L)
+    out["G"] = reconstruction_matrix(np.linspace(-11, 11, 41), (-11.2, 11.2), 128)
+    out["phases"] = random_phases(16, 7, [0, 1, 2, 5])
+    out["phases_c1_head"] = random_phases(4096, 20261019, [0, 7])[:256]
+    return out
+
+
+def square_pipeline():
+    """Full reference stochastic pipeline on a 16x16 square lattice."""
+    m = lattices.square_lattice(16, seed=99)
+    model = ModelBundle(m.H, m.S, velocity=m.velocity)
+    cfg = RunConfig(energy_eV=np.linspace(-9, 9, 19), time_fs=[0., 1., 2., 3.], solver="stochastic-kpm",
+                    kernel="jackson", axes=("x",), spectral_bounds=(-11.5, 11.5), n_moments=64, nsamples=8,
+                    sample_batch=4, statistics_block=2, include_vac=False, stochastic_method="stepwise",
+                    cpu_kernel="cpp", seed=515)
+    ops = build_operators(model, cfg)
+    blocks = list(iter_stochastic_blocks(ops, cfg, "stepwise"))
+    out = {"H_digest": np.array(digest(m.H)), "V_digest": np.array(digest(m.velocity["x"]))}
+    for blk in blocks:
+        for k, v in {**blk.static, **blk.arrays}.items():
+            out["arr/" + k] = np.asarray(v)
+    return out
+
+
+def c1_case():
+    """Config-1 lattice: 64x64 square, R=8 phases, M=512 moments, short MSD."""
+    m = lattices.square_lattice(64)
+    model = ModelBundle(m.H, m.S, velocity=m.velocity)
+    cfg = RunConfig(energy_eV=np.linspace(-11, 11, 201), time_fs=[0., 1., 2., 3.], solver="stochastic-kpm",
+                    kernel="jackson", axes=("x",), spectral_bounds=(-11.2, 11.2), n_moments=512,
+                    include_vac=False, stochastic_method="stepwise", cpu_kernel="cpp", omp_threads=8)
+    ops = build_operators(model, cfg)
+    B = random_phases(m.n, 20261019, range(8))
+    c, a = scaling(cfg)
+    out = {"H_digest": np.array(digest(m.H)), "V_digest": np.array(digest(m.velocity["x"]))}
+    out["moments"] = ops.native.moments(B, 512, c, a)
+    dos, nums, diag = stepwise_samples(ops, cfg, B)
+    out["dos"] = dos
+    out["msd"] = nums["msd_A2/commutator"]
+    return out
+
+
+def diamond_case():
+    m = lattices.diamond_sp3(cells=2)
+    model = ModelBundle(m.H, m.S, composite=m.composite, atom_slices=m.atom_slices)
+    cfg = RunConfig(energy_eV=np.linspace(-8, 6, 8), time_fs=[0., .5, 1.], solver="stochastic-kpm",
+                    kernel="jackson", axes=("x", "y", "z"), spectral_bounds=(-40., 40.), n_moments=32,
+                    include_vac=False, stochastic_method="stepwise", cpu_kernel="cpp", metric_rtol=1e-12,
+                    preconditioner="block-jacobi", segment_fs=.5, omp_threads=8)
+    ops = build_operators(model, cfg)
+    sampler = MetricSampler(ops.metric, cfg)
+    xi = random_phases(m.n, 3, [0, 1])
+    c, a = scaling(cfg)
+    out = {"H_digest": np.array(digest(m.H)), "S_digest": np.array(digest(m.S)),
+           "bounds": np.asarray(cfg.spectral_bounds)}
+    out["xi"] = xi
+    out["sample_coeff"] = np.asarray(sampler.coeff)
+    out["sample_center"] = sampler.center
+    out["sample_half"] = sampler.half
+    out["sample"] = sampler.transform(xi)
+    B = xi  # unit-modulus phases drive the transport checks below
+    out["B"] = B
+    out["moments"] = ops.native.moments(B, 32, c, a)
+    out["v_cov_y"] = ops.native.v_cov([0., 1., 0.], B)
+    dos, nums, _ = stepwise_samples(ops, cfg, B)
+    out["dos"] = dos
+    out["msd"] = nums["msd_A2/commutator"]
+    out["metric_calls"] = ops.metric.diagnostics()["calls"]
+    return out
+
+
+def main():
+    cases = {}
+    for kind in ("velocity", "position", "composite"):
+        for pre in ("diagonal", "block-jacobi"):
+            cases[f"engine_{kind}_{pre}"] = engine_case(kind, pre)
+    cases["pcg_known"] = pcg_known()
+    cases["host_formulas"] = host_formulas()
+    cases["square16_pipeline"] = square_pipeline()
+    cases["c1_square64"] = c1_case()
+    cases["diamond2"] = diamond_case()
+    for name, arrays in cases.items():
+        np.savez_compressed(HERE / f"{name}.npz", **arrays)
+        print(name, sum(np.asarray(v).nbytes for v in arrays.values()), "bytes")
+
+
+if __name__ == "__main__":
+    main()

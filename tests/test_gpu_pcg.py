@@ -1,0 +1,87 @@
+"""Batched device PCG vs the reference's known answers and failure reports."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from tests.helpers import assert_rel, golden
+
+pytestmark = pytest.mark.gpu
+
+
+def metric(S, blocks=(), rtol=2e-13, maxiter=1000, policy="fixed"):
+    from kubomsd_b200.native import B200Metric
+    from tests.gpu_util import controls
+    cfg = controls(rtol, policy=policy)
+    cfg.metric_maxiter = maxiter
+    S = sp.csr_matrix(S, dtype=complex)
+    return B200Metric(S, S.diagonal().real.copy(), list(blocks), cfg), cfg
+
+
+def test_one_jacobi_step_known_answer(cuda):
+    # One Jacobi-preconditioned CG step from p = (1, .5): y = (15/17, 15/34).
+    m, cfg = metric(np.array([[1., .2], [.2, 2.]]))
+    cfg.metric_rtol, cfg.metric_maxiter = .5, 1
+    y, rep = m.solve(np.ones((2, 1)), cfg)
+    np.testing.assert_allclose(y[:, 0], [15 / 17, 15 / 34], rtol=1e-14, atol=1e-14)
+    assert rep.iterations.tolist() == [1] and rep.converged.tolist() == [True]
+    assert 1e-12 < rep.relative_residual[0] < .5
+
+
+def test_failure_report_matches_reference(cuda):
+    from kubomsd_b200.errors import NumericalError
+    d = golden("pcg_known")
+    m, cfg = metric(np.array([[1, .2j], [-.2j, 2]]), maxiter=1)
+    with pytest.raises(NumericalError) as failed:
+        m.solve(np.array([[0, 1], [0, 1]], complex), cfg)
+    assert str(failed.value) == str(d["fail_message"])
+    assert failed.value.diagnostics["converged"] == d["fail_converged"].tolist()
+    assert failed.value.diagnostics["iterations"] == d["fail_iterations"].tolist()
+
+
+@pytest.mark.parametrize("pre", ["diagonal", "block-jacobi"])
+def test_extreme_column_scales(cuda, pre):
+    import scipy.linalg as la
+    d = golden("pcg_known")
+    S, B = d["scaled_S"], d["scaled_B"]
+    blocks = [] if pre == "diagonal" else [(a, b, la.cholesky(S[a:b, a:b], lower=True))
+                                            for a, b in ((0, 3), (3, 7), (7, 11))]
+    m, cfg = metric(S, blocks)
+    y, rep = m.solve(B, cfg)
+    for j in range(4):
+        assert_rel(y[:, j], d[f"scaled_{pre}"][:, j], 1e-11, f"column {j}")
+    np.testing.assert_array_equal(y[:, 0], 0)
+    assert rep.converged.all()
+    assert np.all(np.abs(rep.iterations - d[f"scaled_{pre}_iterations"]) <= 1)
+
+
+@pytest.mark.parametrize("policy", ["fixed", "adaptive"])
+def test_true_residual_refresh(cuda, policy):
+    d = golden("pcg_known")
+    n = 96
+    T = sp.diags([-np.ones(n - 1), 2.03 * np.ones(n), -np.ones(n - 1)], [-1, 0, 1], format="csr", dtype=complex)
+    m, cfg = metric(T, rtol=1e-11, policy=policy)
+    y, rep = m.solve(d["tri_B"], cfg)
+    want = d["tri"] if policy == "fixed" else d["tri_adaptive"]
+    assert_rel(y, want, 1e-9, policy)
+    assert np.all(rep.relative_residual <= 1e-11)
+    st = m.stats()
+    assert st.true_residual_refreshes >= 1
+    if policy == "fixed":
+        assert abs(st.true_residual_refreshes - int(d["tri_refreshes"])) <= 1
+
+
+def test_unrepresentable_solution_is_rejected(cuda):
+    from kubomsd_b200.errors import NumericalError
+    m, cfg = metric(.25 * np.eye(2))
+    with pytest.raises(NumericalError, match="representable") as failed:
+        m.solve(np.array([[1e308, 1.], [1., 1.]], dtype=complex), cfg)
+    assert failed.value.diagnostics["converged"] == [False, True]
+
+
+def test_extreme_finite_rhs_keeps_representable_solution(cuda):
+    m, cfg = metric(np.eye(2))
+    y, rep = m.solve(np.array([[complex(1.3e308, 1.3e308)], [1. + 0j]]), cfg)
+    assert np.isfinite(y).all()
+    np.testing.assert_allclose(y[0].real / 1.3e308, [1.], rtol=1e-14)
+    np.testing.assert_allclose(y[1], [1.], rtol=1e-14, atol=0)
+    assert rep.converged.tolist() == [True]
