@@ -12,6 +12,8 @@
 //    then the same step kernel reading the solved operand (FP64 only).
 #include <algorithm>
 #include <atomic>
+#include <map>
+#include <mutex>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -74,6 +76,25 @@ int grid_for(int64_t rows, const RowMap &mp) {
     const int64_t need = (rows + mp.gpc - 1) / mp.gpc;
     const int64_t cap = (int64_t)sm_count() * 8;  // 8 CTAs of 256 threads per SM
     return (int)std::max<int64_t>(1, std::min(need, cap));
+}
+int wave_grid(const void *kernel, size_t smem, int64_t rows, const RowMap &mp) {
+    static std::mutex lock;
+    static std::map<std::pair<const void *, size_t>, int> cache;
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> g(lock);
+        auto it = cache.find({kernel, smem});
+        if (it != cache.end()) {
+            per_sm = it->second;
+        } else {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, smem) != cudaSuccess ||
+                per_sm < 1)
+                per_sm = 1;
+            cache[{kernel, smem}] = per_sm;
+        }
+    }
+    const int64_t need = (rows + mp.gpc - 1) / mp.gpc;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sm_count() * per_sm));
 }
 int mu_for(const RowMap &mp) {
     const int per = (mp.U + mp.G - 1) / mp.G;

@@ -37,6 +37,9 @@ int sm_count();
 void count_launch(int64_t n = 1);
 // Grid for a row-group kernel over `rows` rows.
 int grid_for(int64_t rows, const RowMap &mp);
+// Grid of one resident wave of `kernel` (occupancy API; cached per kernel and
+// shared-memory size), capped by the row groups needed.
+int wave_grid(const void *kernel, size_t smem, int64_t rows, const RowMap &mp);
 // Units per thread bucket {1,2,4,8}; 0 when too wide.
 int mu_for(const RowMap &mp);
 size_t reduce_smem(const RowMap &mp, int C);

@@ -160,23 +160,35 @@ int v_cov(E *e, const double *dir, const double2 *B, double2 *out, int64_t b, co
 }
 
 // ---------------------------------------------------------------- step launch
-template <class T, int MODE, bool IH, bool IV>
-int launch_step(E *e, StepArgs<T> &a, cudaStream_t s) {
-    const int mu = mu_for(a.mp);
-    const int grid = grid_for(a.n, a.mp);
+// One resident wave: the grid is the number of CTAs the SMs hold at once for
+// this kernel (occupancy API), capped by the rows to cover.  Fixed per kernel
+// and shape, so row ownership — and with it every reduction order — is
+// reproducible run to run.
+template <class T, int MU, int MODE, bool IH, bool IV>
+int launch_step_mu(E *e, StepArgs<T> &a, cudaStream_t s) {
+    const auto kern = cheb_step_kernel<T, MU, MODE, IH, IV>;
     const size_t sm = reduce_smem(a.mp, Unit<T>::C);
+    const int grid = wave_grid((const void *)kern, sm, a.n, a.mp);
     if (MODE == MODE_DIRECT || MODE == MODE_DOUBLING) {
         if (e->red.ensure(grid, a.mp.U * Unit<T>::C, 2)) return KMSD_ECUDA;
         a.partial = e->red.part();
         a.ticket = e->red.tick();
     }
-    switch (mu) {
-        case 1: cheb_step_kernel<T, 1, MODE, IH, IV><<<grid, kThreads, sm, s>>>(a); break;
-        case 2: cheb_step_kernel<T, 2, MODE, IH, IV><<<grid, kThreads, sm, s>>>(a); break;
-        case 4: cheb_step_kernel<T, 4, MODE, IH, IV><<<grid, kThreads, sm, s>>>(a); break;
-        case 8: cheb_step_kernel<T, 8, MODE, IH, IV><<<grid, kThreads, sm, s>>>(a); break;
+    kern<<<grid, kThreads, sm, s>>>(a);
+    return KMSD_OK;
+}
+
+template <class T, int MODE, bool IH, bool IV>
+int launch_step(E *e, StepArgs<T> &a, cudaStream_t s) {
+    int rc;
+    switch (mu_for(a.mp)) {
+        case 1: rc = launch_step_mu<T, 1, MODE, IH, IV>(e, a, s); break;
+        case 2: rc = launch_step_mu<T, 2, MODE, IH, IV>(e, a, s); break;
+        case 4: rc = launch_step_mu<T, 4, MODE, IH, IV>(e, a, s); break;
+        case 8: rc = launch_step_mu<T, 8, MODE, IH, IV>(e, a, s); break;
         default: return fail(KMSD_EINVAL, "too many columns for one engine call");
     }
+    if (rc) return rc;
     count_launch();
     KMSD_CUDA(cudaGetLastError());
     return KMSD_OK;
