@@ -90,6 +90,7 @@ class RunConfig:
     rho_abs: float = 0.
     rho_rel: float = 1e-12
     memory_limit_gb: float = 4.
+    output_npz: bool = False
     precision: str = "fp64"
     moment_doubling: bool = False
 

@@ -120,6 +120,100 @@ def stepwise_samples(ops, cfg, samples):
         "seconds": time.perf_counter() - t0, "device_resident": True}
 
 
+def spectral_samples(ops, cfg, samples):
+    """Segmented trace-first Chebyshev product VAC (spectral.py:15-53).
+
+    Per segment the anchors are propagated on the device, the left chain
+    T_j(Ht) c (j < L+K) and the right chains T_k(Ht) v_a (k <= K) are built by
+    the engine, the velocity is applied to the right chains on the device, and
+    the correlation tables tables[b, j, k] = sum_n conj(left[j,n,b]) cov[k,n,b]
+    are one batched complex GEMM per axis on the device.  The per-node Bessel
+    contraction, product rule T_l T_p = (T_l+p + T_|l-p|)/2, Jackson projection
+    and the M/D recurrence run in FP64 on the host in the reference's order.
+    """
+    from .config import resolve_time_grid
+    torch = _torch()
+    x = samples if isinstance(samples, torch.Tensor) else torch.from_numpy(
+        np.ascontiguousarray(samples, dtype=np.complex128))
+    x = x.to("cuda", torch.complex128).contiguous()
+    n, nb = x.shape
+    na, ne, nt, L = len(cfg.axes), len(cfg.energy_eV), len(cfg.time_fs), cfg.n_moments
+    t0 = time.perf_counter()
+    dos = projected_quadratic(x, ops, cfg)
+    keys = ("msd_A2/vac_integral", "diffusion_A2_per_fs/vac_integral", "vac_A2_per_fs2/vac_integral")
+    output = {k: np.zeros((nb, na, nt, ne)) for k in keys}
+    times = np.unique(np.r_[resolve_time_grid(cfg.time_fs[-1], cfg.integration_dt_fs), cfg.time_fs])
+    output_indices = {float(t): j for j, t in enumerate(cfg.time_fs)}
+    G = kpm.reconstruction_matrix(cfg.energy_eV, cfg.spectral_bounds, L)
+    c_anchor = x
+    v_anchor = [ops.apply_v_action(a, x) for a in cfg.axes]
+    anchor, next_anchor, tables = 0., -1., None
+    maxorder = segments = 0
+    maxnorm = 0.
+    c, a = kpm.scaling(cfg)
+    M = np.zeros((nb, na, ne))
+    D = np.zeros_like(M)
+    previous, prev_t = None, 0.
+    for t in times:
+        if tables is None or t > next_anchor + 1e-14:
+            new_anchor = 0. if tables is None else float(prev_t)
+            if new_anchor > anchor:
+                both = torch.cat([c_anchor] + v_anchor, dim=1).contiguous()
+                both, report = propagate(both, new_anchor - anchor, ops, cfg)
+                maxnorm = max(maxnorm, report["relative_S_norm_drift"])
+                c_anchor = both[:, :nb].contiguous()
+                v_anchor = [both[:, (i + 1) * nb:(i + 2) * nb].contiguous() for i in range(na)]
+            anchor = new_anchor
+            next_anchor = min(max(anchor + cfg.segment_fs, float(t)), float(times[-1]))
+            coeff, _ = kpm.bessel_coefficients(next_anchor - anchor, cfg)
+            K = len(coeff) - 1
+            maxorder = max(maxorder, K)
+            estimate = 16 * nb * (n * (L + 2 * K + 1) + na * (L + K) * (K + 1)) + 24 * nb * na * nt * ne
+            if estimate > cfg.memory_limit_gb * 1024 ** 3:
+                raise NumericalError("spectral workspace exceeds memory budget; reduce sample_batch/segment_fs or "
+                                     "increase explicit budget")
+            left = ops.native.chain(c_anchor, L + K, c, a)           # (L+K, n, nb) on the device
+            lconj = left.permute(2, 0, 1).conj()                     # (nb, L+K, n)
+            tables = []
+            for ai, axis in enumerate(cfg.axes):
+                right = ops.native.chain(v_anchor[ai], K + 1, c, a)  # (K+1, n, nb)
+                cov = ops.apply_v_cov(axis, right.permute(1, 0, 2).reshape(n, -1).contiguous())
+                cov = cov.reshape(n, K + 1, nb)                      # (n, K+1, nb)
+                tables.append(torch.matmul(lconj, cov.permute(2, 0, 1)).cpu().numpy())  # (nb, L+K, K+1)
+                del right, cov
+            del left, lconj
+            segments += 1
+        b, _ = kpm.bessel_coefficients(float(t - anchor), cfg)
+        Kt = len(b) - 1
+        if Kt > tables[0].shape[-1] - 1:
+            raise NumericalError("internal spectral propagation order exceeded segment allocation")
+        vac = np.empty((nb, na, ne))
+        l_ = np.arange(L)[:, None]
+        p_ = np.arange(Kt + 1)[None, :]
+        for ai, table in enumerate(tables):
+            q = table[:, :, :Kt + 1] @ b
+            moments = np.sum(.5 * (q[:, l_ + p_] + q[:, np.abs(l_ - p_)]) * b.conj()[None, None, :], axis=2).real
+            vac[:, ai, :] = moments @ G.T
+        if previous is not None:
+            h = float(t - prev_t)
+            M = M + 2 * h * D + h * h / 3 * (2 * previous + vac)
+            D = D + h / 2 * (previous + vac)
+        if float(t) in output_indices:
+            j = output_indices[float(t)]
+            output["msd_A2/vac_integral"][:, :, j, :] = M
+            output["diffusion_A2_per_fs/vac_integral"][:, :, j, :] = D
+            output["vac_A2_per_fs2/vac_integral"][:, :, j, :] = vac
+        previous, prev_t = vac, t
+    if not cfg.include_vac:
+        output.pop("vac_A2_per_fs2/vac_integral")
+    return dos, output, {"algorithm": "segmented trace-first Chebyshev product VAC", "segments": segments,
+                         "max_propagation_order": maxorder, "max_relative_S_norm_drift": maxnorm,
+                         "integration_scheme": "piecewise linear VAC, simultaneous M/D recurrence",
+                         "internal_nodes": len(times), "integration_dt_fs": cfg.integration_dt_fs,
+                         "integration_validation": "UNVERIFIED until step-size convergence",
+                         "seconds": time.perf_counter() - t0, "device_resident": "chains, velocity, tables"}
+
+
 class Sampler:
     """Metric-corrected random vectors D^-1/2 p(W) xi (metric/sampling.py:11-46)."""
 
@@ -143,17 +237,27 @@ def sample_metric(seed, sample_ids, ops, cfg):
 
 def _quantity_keys(cfg, method):
     keys = ["msd_A2/commutator"] if method == "stepwise" else []
+    if method == "spectral" or cfg.include_vac:
+        keys += ["msd_A2/vac_integral", "diffusion_A2_per_fs/vac_integral"]
+        if cfg.include_vac:
+            keys += ["vac_A2_per_fs2/vac_integral"]
     if len(cfg.time_fs) > 1:
         keys += ["diffusion_A2_per_fs/msd_gradient"]
     return keys
 
 
+def choose_stochastic_method(config):
+    """'auto' resolves to stepwise (src/kubo_msd/dispatch.py:17-19)."""
+    return "stepwise" if config.stochastic_method == "auto" else config.stochastic_method
+
+
 def iter_stochastic_blocks(ops, config, method="stepwise", samples=None, parallel=None, bounds_report=None):
     """Stochastic transport blocks with the reference's array names and
-    statistics (stochastic.py:122-228); stepwise method, VAC off."""
-    if method != "stepwise" or getattr(config, "include_vac", False):
-        raise BackendUnavailable("the B200 backend implements the stepwise commutator method without the "
-                                 "spectral VAC route (use stochastic_method='stepwise', include_vac=False)")
+    statistics (stochastic.py:122-228): stepwise commutator MSD with the
+    optional spectral VAC route, or the spectral method alone."""
+    if method not in ("stepwise", "spectral"):
+        raise BackendUnavailable(f"unsupported stochastic method {method!r}")
+    primary = "commutator" if method == "stepwise" else "vac_integral"
     ctx = parallel or ParallelContext()
     cfg = config
     if bounds_report is None:
@@ -179,9 +283,17 @@ def iter_stochastic_blocks(ops, config, method="stepwise", samples=None, paralle
                 last = min(first + cfg.sample_batch, end_id)
                 ids = np.arange(first, last)
                 B = sample_metric(cfg.seed, ids, ops, cfg) if samples is None else samples[:, first:last]
-                dos, nums, diag = stepwise_samples(ops, cfg, B)
+                if method == "stepwise":
+                    dos, nums, diag = stepwise_samples(ops, cfg, B)
+                    if cfg.include_vac:
+                        _, extra, extra_diag = spectral_samples(ops, cfg, B)
+                        nums.update(extra)
+                        diag["additional_vac_path"] = extra_diag
+                        diag["additional_cost_recorded"] = True
+                else:
+                    dos, nums, diag = spectral_samples(ops, cfg, B)
                 if len(cfg.time_fs) > 1:
-                    nums["diffusion_A2_per_fs/msd_gradient"] = kpm.msd_gradient(cfg.time_fs, nums["msd_A2/commutator"],
+                    nums["diffusion_A2_per_fs/msd_gradient"] = kpm.msd_gradient(cfg.time_fs, nums["msd_A2/" + primary],
                                                                                axis=2)
                 diagnostics.append(diag)
                 ids_used.extend(ids.tolist())
@@ -214,7 +326,8 @@ def iter_stochastic_blocks(ops, config, method="stepwise", samples=None, paralle
                   "sample_count": np.array(ns), "sample_ids": np.arange(ns)}
         if stderr_dos is not None:
             static["stderr_dos_states_per_eV"] = stderr_dos
-        metadata = {"primary_estimator": "commutator", "primary_diffusion_estimator": "msd_gradient",
+        metadata = {"primary_estimator": primary,
+                    "primary_diffusion_estimator": "msd_gradient" if method == "stepwise" else "vac_integral",
                     "resolved_config": cfg.as_dict() if hasattr(cfg, "as_dict") else {}, "spectral_report":
                     bounds_report, "dos_floor": threshold, "statistical_method": stat,
                     "sample_generator": "NumPy PCG64 SeedSequence([seed,sample_id]); unit modulus complex phases",
@@ -239,9 +352,12 @@ def iter_stochastic_blocks(ops, config, method="stepwise", samples=None, paralle
         if ctx.root:
             valid, reason, static, metadata = normalized
             for estimator in {k.split("/")[-1] for k in keys}:
+                r = reason.copy()
+                if estimator == "vac_integral":
+                    r |= REASON_INTEGRATION_UNVERIFIED
                 dims = (len(cfg.axes), stop - start, len(cfg.energy_eV))
                 arrays["valid/" + estimator] = np.broadcast_to(valid, dims).copy()
-                arrays["reason_code/" + estimator] = np.broadcast_to(reason.copy(), dims).copy()
+                arrays["reason_code/" + estimator] = np.broadcast_to(r, dims).copy()
             yield TransportBlock(start, cfg.time_fs[start:stop], arrays, static if start == 0 else {},
                                  metadata if start == 0 else {})
         else:

@@ -89,7 +89,7 @@ class Metric:
     def solve(self, B, rtol, atol, maxiter):
         """Batched PCG, column by column semantics of Metric::solve
         (cpp/native.cpp:313-452)."""
-        B = dense(B) if np.iscomplexobj(B) or True else B
+        B = dense(B)
         if B.shape[0] != self.n or rtol < 0 or atol < 0 or maxiter < 1:
             raise ValueError("invalid metric RHS shape/tolerances")
         n, b = B.shape
@@ -470,3 +470,73 @@ def sampler_coefficients(S, tol=1e-10, max_order=4096):
         if order >= max_order:
             break
     raise ValueError("metric inverse sqrt polynomial failed sampling tolerance")
+
+
+def resolve_time_grid(tmax, dt):
+    """Uniform grid 0..tmax with tmax appended (src/kubo_msd/config.py:19-24)."""
+    t = np.arange(int(np.floor(tmax / dt)) + 1, dtype=float) * dt
+    if t[-1] < tmax and not np.isclose(t[-1], tmax, rtol=0, atol=8 * np.spacing(max(tmax, dt))):
+        t = np.append(t, tmax)
+    else:
+        t[-1] = tmax
+    return t
+
+
+def spectral_samples(engine, samples, energies, times_out, bounds, n_moments, axes_vectors, integration_dt,
+                     segment_fs=1., tol=1e-12, max_order=4096, include_vac=True):
+    """Segmented trace-first Chebyshev product VAC
+    (src/kubo_msd/solvers/spectral.py:15-53): returns (dos, outputs)."""
+    x = np.asarray(samples, complex)
+    n, nb = x.shape
+    na, ne, nt, L = len(axes_vectors), len(energies), len(times_out), n_moments
+    dos = projected_quadratic(engine, x, energies, bounds, n_moments)
+    keys = ("msd_A2/vac_integral", "diffusion_A2_per_fs/vac_integral", "vac_A2_per_fs2/vac_integral")
+    out = {k: np.zeros((nb, na, nt, ne)) for k in keys}
+    times = np.unique(np.r_[resolve_time_grid(times_out[-1], integration_dt), times_out])
+    index = {float(t): j for j, t in enumerate(times_out)}
+    G = reconstruction(energies, bounds, L)
+    c, a = scaling(bounds)
+    c_anchor = x
+    v_anchor = [engine.solve(engine.v_cov(list(d), x)) for d in axes_vectors]
+    anchor, next_anchor, tables = 0., -1., None
+    M = np.zeros((nb, na, ne))
+    D = np.zeros_like(M)
+    previous, prev_t = None, 0.
+    for t in times:
+        if tables is None or t > next_anchor + 1e-14:
+            new_anchor = 0. if tables is None else float(prev_t)
+            if new_anchor > anchor:
+                both, _ = propagate(engine, np.concatenate([c_anchor] + v_anchor, axis=1), new_anchor - anchor,
+                                    bounds, segment_fs, tol, max_order)
+                c_anchor = both[:, :nb]
+                v_anchor = [both[:, (i + 1) * nb:(i + 2) * nb] for i in range(na)]
+            anchor = new_anchor
+            next_anchor = min(max(anchor + segment_fs, float(t)), float(times[-1]))
+            coeff, K = bessel_coefficients(next_anchor - anchor, bounds, tol, max_order)
+            left = engine.chain(c_anchor, L + K, c, a)
+            tables = []
+            for ai, d in enumerate(axes_vectors):
+                right = engine.chain(v_anchor[ai], K + 1, c, a)
+                cov = engine.v_cov(list(d), right.transpose(1, 0, 2).reshape(n, -1)).reshape(n, K + 1, nb)
+                tables.append(np.einsum("jnb,knb->bjk", left.conj(), cov.transpose(1, 0, 2)))
+        b, Kt = bessel_coefficients(float(t - anchor), bounds, tol, max_order)
+        vac = np.empty((nb, na, ne))
+        l_ = np.arange(L)[:, None]
+        p_ = np.arange(Kt + 1)[None, :]
+        for ai, table in enumerate(tables):
+            q = table[:, :, :Kt + 1] @ b
+            moments = np.sum(.5 * (q[:, l_ + p_] + q[:, np.abs(l_ - p_)]) * b.conj()[None, None, :], axis=2).real
+            vac[:, ai, :] = moments @ G.T
+        if previous is not None:
+            h = float(t - prev_t)
+            M = M + 2 * h * D + h * h / 3 * (2 * previous + vac)
+            D = D + h / 2 * (previous + vac)
+        if float(t) in index:
+            j = index[float(t)]
+            out["msd_A2/vac_integral"][:, :, j, :] = M
+            out["diffusion_A2_per_fs/vac_integral"][:, :, j, :] = D
+            out["vac_A2_per_fs2/vac_integral"][:, :, j, :] = vac
+        previous, prev_t = vac, t
+    if not include_vac:
+        out.pop("vac_A2_per_fs2/vac_integral")
+    return dos, out

@@ -44,6 +44,7 @@ from kubo_msd.metric.solve import MetricSolver  # noqa: E402
 from kubo_msd.operators.velocity import build_operators  # noqa: E402
 from kubo_msd.solvers.chebyshev import bessel_coefficients, scaling  # noqa: E402
 from kubo_msd.solvers.stepwise import propagate, stepwise_samples  # noqa: E402
+from kubo_msd.solvers.spectral import spectral_samples  # noqa: E402
 from kubo_msd.solvers.stochastic import iter_stochastic_blocks  # noqa: E402
 from kubo_msd.kernels.energy import jackson_coefficients, reconstruction_matrix  # noqa: E402
 
@@ -138,6 +139,11 @@ def engine_case(kind, precond):
     dos, nums, _ = stepwise_samples(ops, cfg, B)
     out["dos"] = dos
     out["msd"] = nums["msd_A2/commutator"]
+    vcfg = replace(cfg, include_vac=True, integration_dt_fs=.01)
+    _, vac, _ = spectral_samples(ops, vcfg, B)
+    for key, value in vac.items():
+        out["spectral/" + key] = value
+    out["integration_dt_fs"] = vcfg.integration_dt_fs
     out["energies"] = np.asarray(cfg.energy_eV)
     out["times"] = np.asarray(cfg.time_fs)
     out["n_moments"] = cfg.n_moments
@@ -206,16 +212,16 @@ def host_formulas():
     return out
 
 
-def square_pipeline():
+def square_pipeline(method="stepwise", include_vac=False):
     """Full reference stochastic pipeline on a 16x16 square lattice."""
     m = lattices.square_lattice(16, seed=99)
     model = ModelBundle(m.H, m.S, velocity=m.velocity)
     cfg = RunConfig(energy_eV=np.linspace(-9, 9, 19), time_fs=[0., 1., 2., 3.], solver="stochastic-kpm",
                     kernel="jackson", axes=("x",), spectral_bounds=(-11.5, 11.5), n_moments=64, nsamples=8,
-                    sample_batch=4, statistics_block=2, include_vac=False, stochastic_method="stepwise",
-                    cpu_kernel="cpp", seed=515)
+                    sample_batch=4, statistics_block=2, include_vac=include_vac, stochastic_method=method,
+                    cpu_kernel="cpp", seed=515, integration_dt_fs=.05)
     ops = build_operators(model, cfg)
-    blocks = list(iter_stochastic_blocks(ops, cfg, "stepwise"))
+    blocks = list(iter_stochastic_blocks(ops, cfg, method))
     out = {"H_digest": np.array(digest(m.H)), "V_digest": np.array(digest(m.velocity["x"]))}
     for blk in blocks:
         for k, v in {**blk.static, **blk.arrays}.items():
@@ -278,6 +284,8 @@ def main():
     cases["pcg_known"] = pcg_known()
     cases["host_formulas"] = host_formulas()
     cases["square16_pipeline"] = square_pipeline()
+    cases["square16_pipeline_vac"] = square_pipeline("stepwise", include_vac=True)
+    cases["square16_pipeline_spectral"] = square_pipeline("spectral", include_vac=False)
     cases["c1_square64"] = c1_case()
     cases["diamond2"] = diamond_case()
     for name, arrays in cases.items():

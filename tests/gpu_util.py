@@ -22,7 +22,14 @@ def engine(H, S, velocity=None, position=None, composite=None, blocks=(), rtol=1
     ops = SimpleNamespace(host_H=H, metric=SimpleNamespace(native=metric), velocity=velocity or {},
                           position=position or {}, composite=composite or {})
     eng = B200Operators(ops, cfg)
-    return metric, eng, SimpleNamespace(native=eng, inner=eng.inner)
+
+    def v_cov(axis, B, config=None):
+        return eng.v_cov(np.eye(3)["xyz".index(axis)], B, config)
+
+    def v_action(axis, B):
+        return metric.solve(v_cov(axis, B), cfg)[0]
+
+    return metric, eng, SimpleNamespace(native=eng, inner=eng.inner, apply_v_cov=v_cov, apply_v_action=v_action)
 
 
 def fixture_engine(d, kind, pre, precision="fp64"):

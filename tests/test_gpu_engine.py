@@ -73,3 +73,21 @@ def test_engine_counters_follow_reference_semantics(cuda):
     eng.series(d["aug"], d["coeff"], float(d["center"]), float(d["half"]), [[1., 0., 0.]])
     assert eng.core.h_calls == 19 + len(d["coeff"]) - 1
     assert eng.core.v_calls == len(d["coeff"]) - 1
+
+
+@pytest.mark.parametrize("pre", PRECONDS)
+@pytest.mark.parametrize("kind", KINDS)
+def test_spectral_vac_matches_reference(cuda, kind, pre):
+    from kubomsd_b200 import stochastic
+    from kubomsd_b200.config import RunConfig
+    from tests.gpu_util import fixture_engine
+    d = golden(f"engine_{kind}_{pre}")
+    _, eng, ops = fixture_engine(d, kind, pre)
+    cfg = RunConfig(energy_eV=d["energies"], time_fs=d["times"], spectral_bounds=tuple(d["bounds"]),
+                    n_moments=int(d["n_moments"]), axes=("x",), segment_fs=float(d["segment_fs"]),
+                    metric_rtol=float(d["rtol"]), include_vac=True, stochastic_method="spectral",
+                    integration_dt_fs=float(d["integration_dt_fs"]), preconditioner=pre)
+    dos, out, diag = stochastic.spectral_samples(ops, cfg, d["B"])
+    assert_rel(dos, d["dos"], 1e-10, "dos")
+    for key in ("msd_A2/vac_integral", "diffusion_A2_per_fs/vac_integral", "vac_A2_per_fs2/vac_integral"):
+        assert_rel(out[key], d["spectral/" + key], 1e-9, key)

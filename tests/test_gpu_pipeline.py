@@ -9,19 +9,22 @@ from tests.helpers import golden
 pytestmark = pytest.mark.gpu
 
 
-def test_square16_pipeline_matches_reference(cuda):
+@pytest.mark.parametrize("name,method,vac", [("square16_pipeline", "stepwise", False),
+                                              ("square16_pipeline_vac", "stepwise", True),
+                                              ("square16_pipeline_spectral", "spectral", False)])
+def test_square16_pipeline_matches_reference(cuda, name, method, vac):
     from kubomsd_b200 import lattices, stochastic
     from kubomsd_b200.config import RunConfig
     from kubomsd_b200.operators import build_operators
     from tests.golden.make_golden_digest import digest
-    d = golden("square16_pipeline")
+    d = golden(name)
     m = lattices.square_lattice(16, seed=99)
     assert digest(m.H) == str(d["H_digest"])
     cfg = RunConfig(energy_eV=np.linspace(-9, 9, 19), time_fs=[0., 1., 2., 3.], axes=("x",),
                     spectral_bounds=(-11.5, 11.5), n_moments=64, nsamples=8, sample_batch=4, statistics_block=2,
-                    include_vac=False, stochastic_method="stepwise", seed=515)
+                    include_vac=vac, stochastic_method=method, seed=515, integration_dt_fs=.05)
     ops = build_operators(m, cfg)
-    blocks = list(stochastic.iter_stochastic_blocks(ops, cfg, "stepwise"))
+    blocks = list(stochastic.iter_stochastic_blocks(ops, cfg, method))
     got = {}
     for blk in blocks:
         got.update(blk.static)

@@ -141,3 +141,14 @@ def test_oracle_matches_compiled_reference_live(seed):
     assert_rel(e.chain(B, 7, .1, 2.), ref.core.chain(B, 7, .1, 2.), 1e-10, "chain")
     y, rep = ref.metric.solve(B, 2e-13, 0., 1000)
     assert_rel(e.metric.solve(B, 2e-13, 0., 1000)[0], y, 1e-11, "solve")
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_oracle_spectral_vac_matches_reference(kind):
+    d = golden(f"engine_{kind}_diagonal")
+    e = oracle_engine(d, kind, "diagonal")
+    dos, out = O.spectral_samples(e, d["B"], d["energies"], d["times"], tuple(d["bounds"]), int(d["n_moments"]),
+                                  [[1., 0., 0.]], float(d["integration_dt_fs"]), segment_fs=float(d["segment_fs"]))
+    assert_rel(dos, d["dos"], 1e-10, "dos")
+    for key, value in out.items():
+        assert_rel(value, d["spectral/" + key], 1e-9, key)
