@@ -217,6 +217,23 @@ int kmsd_engine_moments(kmsd_engine e, const void *b_in, double *mu, int64_t b,
                         int64_t length, double center, double half, int flags,
                         void *stream);
 
+/* The moments of kmsd_engine_moments, computed without allocating device
+ * memory; no counterpart in the reference.  For callers that cannot call
+ * cudaMalloc where they need moments: serving loops that must not stall on
+ * the device synchronisation of cudaMalloc/cudaFree, frameworks that keep
+ * all device memory in their own pool, code that must not fail with
+ * out-of-memory mid-run.  Orthogonal-basis engines (S = I) only; FP64, or
+ * MIXED once an allocating call has created the complex64 copy of H.  The
+ * workspace is one static 64 MiB device block per GPU (part of the library
+ * image, held until exit); calls that need more are rejected with
+ * KMSD_EINVAL.  The first call on a GPU looks up the block's address; make it
+ * before any stream capture.  All calls on a GPU share the block: calls that
+ * overlap on the GPU race, so keep them on one stream.  Asynchronous on
+ * `stream`; mu is device memory (length, b). */
+int kmsd_engine_moments_noalloc(kmsd_engine e, const void *b_in, double *mu,
+                                int64_t b, int64_t length, double center,
+                                double half, int flags, void *stream);
+
 /* Reference counters h_calls / v_calls (cpp/native.cpp:718-719). */
 int kmsd_engine_counters(kmsd_engine e, int64_t *h_calls, int64_t *v_calls);
 

@@ -64,6 +64,7 @@ SIGNATURES = {
     "kmsd_engine_series": (C.c_int, [P, P, P, I64, PD, I64, D, D, PD, I64, P]),
     "kmsd_engine_chain": (C.c_int, [P, P, P, I64, I64, D, D, P]),
     "kmsd_engine_moments": (C.c_int, [P, P, PD, I64, I64, D, D, C.c_int, P]),
+    "kmsd_engine_moments_noalloc": (C.c_int, [P, P, PD, I64, I64, D, D, C.c_int, P]),
     "kmsd_engine_counters": (C.c_int, [P, PI64, PI64]),
     "kmsd_engine_failure_report": (C.c_int, [P, C.POINTER(SolveReport), I64, PI64]),
     "kmsd_engine_inner": (C.c_int, [P, P, P, P, I64, P]),

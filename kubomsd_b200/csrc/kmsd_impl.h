@@ -8,6 +8,7 @@
 #include <string>
 #include <vector>
 
+#include "kmsd.h"
 #include "kmsd_common.cuh"
 
 namespace kmsd {
@@ -118,6 +119,8 @@ struct kmsd_metric_s {
               kmsd_solve_report *report, cudaStream_t s, int *status = nullptr, void *fail_report = nullptr);
 };
 
+struct FailReportFull;
+
 // Per-column device failure report for asynchronous solves.
 struct FailReport {
     int64_t ncols;
@@ -132,4 +135,23 @@ struct FailReportFull {
     int64_t iterations[kMaxReportCols];
     double true_residual[kMaxReportCols];
     double relative_residual[kMaxReportCols];
+};
+
+// ------------------------------------------------------------------ engine
+struct kmsd_engine_s {
+    kmsd_csr_s *H = nullptr;
+    kmsd_metric_s *M = nullptr;
+    int vel_kind[3] = {-1, -1, -1};
+    kmsd_csr_s *vel[9] = {};
+    double rtol = 1e-10, atol = 0., hbar = 0.6582119569509067;
+    int maxiter = 1000;
+    int precision = KMSD_FP64;
+    int64_t h_calls = 0, v_calls = 0;
+    bool identity = false;
+    kmsd::DevBuf ta, tb, bra, hx, t1, t2, t3, t4, t5, psi, vc, inj[3], outw;
+    kmsd::DevBuf status;  // int[4]: [0] code, [1] report claim, [2] series nonfinite
+    kmsd::DevBuf report;  // FailReportFull
+    kmsd::DevBuf dots;    // double2[512]
+    kmsd::Reducer red;
+    FailReportFull last{};
 };

@@ -1,0 +1,218 @@
+// KPM moments without any device allocation.
+//
+// Some callers cannot call cudaMalloc at the point where they need moments.
+// Examples: a serving loop that must not stall other streams on the implicit
+// device synchronisation of cudaMalloc/cudaFree; a host framework that owns
+// every byte of device memory through its own pool and budget; code that must
+// not hit an out-of-memory failure halfway through a run.  For them,
+// kmsd_engine_moments_noalloc computes the same moments as
+// kmsd_engine_moments on an orthogonal-basis engine (S = I).  Its workspace is
+// a fixed block of device memory that is part of the library image: the
+// vector buffers of the Chebyshev recurrence, the reduction partials and the
+// reduction ticket all live in `g_moments_scratch` below.
+//
+// Properties a caller must know:
+//  * the block is 64 MiB per GPU, allocated when the library's module is
+//    loaded on that GPU and held until the process exits;
+//  * calls whose buffers would not fit are rejected with KMSD_EINVAL and a
+//    message naming the bytes needed; kmsd_engine_moments has no such limit;
+//  * the first call on each GPU looks up the block's device address (once
+//    per device, under a lock); make that first call before any stream
+//    capture;
+//  * every call on a GPU uses the same block and leaves its contents
+//    behind.  The call clears what must start at zero, so the contents left by
+//    an earlier call are harmless.  Two calls that overlap on the GPU, on
+//    different streams or from different threads, race on the block: order
+//    them on one stream or serialise them;
+//  * the call is asynchronous on `stream`: mu is complete when the stream
+//    reaches the end of the call's work;
+//  * a mixed-precision engine needs the complex64 copy of H, which the first
+//    allocating call (kmsd_engine_moments / series / chain) creates; without
+//    it the call is rejected rather than allocating.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "kmsd.h"
+#include "kmsd_impl.h"
+#include "kmsd_kernels.cuh"
+
+using namespace kmsd;
+
+// The workspace of kmsd_engine_moments_noalloc (see the file comment).
+static constexpr size_t kMomentsScratchBytes = size_t(64) << 20;
+static __device__ __align__(256) unsigned char g_moments_scratch[kMomentsScratchBytes];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_lock;
+void *g_scratch_address[kMaxDevices] = {};
+
+// Device address of g_moments_scratch on the current device.  In host code the
+// symbol names a host-side stand-in, not device memory, so its address is
+// looked up with cudaGetSymbolAddress once per device and cached.
+int scratch_address(void **out) {
+    int dev = 0;
+    KMSD_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(KMSD_EINVAL, "device ordinal out of range for the moments scratch");
+    std::lock_guard<std::mutex> guard(g_scratch_lock);
+    if (g_scratch_address[dev] == nullptr) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_moments_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_moments_scratch)");
+        g_scratch_address[dev] = p;
+    }
+    *out = g_scratch_address[dev];
+    return KMSD_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+template <class T, int MU, int MODE>
+int occupancy_grid(int64_t n, const RowMap &mp, size_t smem, int *grid) {
+    int per_sm = 0;
+    KMSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, cheb_step_kernel<T, MU, MODE, true, false>, kThreads, smem));
+    if (per_sm < 1) per_sm = 1;
+    const int64_t need = (n + mp.gpc - 1) / mp.gpc;
+    *grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sm_count() * per_sm));
+    return KMSD_OK;
+}
+
+template <class T, int MU>
+int run(kmsd_engine_s *e, const double2 *B, double *mu, int64_t b, int64_t length, double center, double half,
+        bool doubling, cudaStream_t s) {
+    using V = typename Unit<T>::vec;
+    constexpr int C = Unit<T>::C;
+    const int64_t n = e->H->n;
+    const int U = (int)((b + C - 1) / C);
+    const RowMap mp = make_map(U, kThreads);
+    const size_t smem = reduce_smem(mp, C);
+    const int ncol = U * C;
+    int g_first = 0, g_rest = 0;
+    int rc = occupancy_grid<T, MU, MODE_DOUBLING>(n, mp, smem, &g_first);
+    if (!rc) rc = occupancy_grid<T, MU, MODE_DIRECT>(n, mp, smem, &g_rest);
+    if (rc) return rc;
+    const int grid = std::max(g_first, g_rest);
+    // scratch layout: ticket | T buffer A | T buffer B | bra (mixed, direct) | partials
+    const size_t vec_bytes = align256((size_t)n * U * sizeof(V));
+    const bool need_bra = C == 2 && !doubling;
+    const size_t off_a = 256, off_b = off_a + vec_bytes, off_bra = off_b + vec_bytes;
+    const size_t off_part = off_bra + (need_bra ? vec_bytes : 0);
+    const size_t need = off_part + align256((size_t)grid * ncol * 2 * sizeof(double2));
+    if (need > kMomentsScratchBytes) {
+        char msg[256];
+        snprintf(msg, sizeof msg,
+                 "kmsd_engine_moments_noalloc: this call needs %zu bytes of scratch but the static block holds "
+                 "%zu bytes (64 MiB); use kmsd_engine_moments for larger blocks",
+                 need, kMomentsScratchBytes);
+        return fail(KMSD_EINVAL, msg);
+    }
+    void *base = nullptr;
+    if ((rc = scratch_address(&base))) return rc;
+    unsigned char *sc = static_cast<unsigned char *>(base);
+    Ticket *ticket = reinterpret_cast<Ticket *>(sc);
+    V *ta = reinterpret_cast<V *>(sc + off_a), *tb = reinterpret_cast<V *>(sc + off_b);
+    V *bra = need_bra ? reinterpret_cast<V *>(sc + off_bra) : nullptr;
+    double2 *partial = reinterpret_cast<double2 *>(sc + off_part);
+    KMSD_CUDA(cudaMemsetAsync(ticket, 0, 256, s));  // the ticket must start at zero
+
+    StepArgs<T> a;
+    std::memset(&a, 0, sizeof(a));
+    a.n = n;
+    a.mp = mp;
+    if constexpr (C == 2) {
+        a.H = CsrView<T>{e->H->ptr, e->H->idx, reinterpret_cast<const T *>(e->H->re32),
+                         e->H->complex_values ? reinterpret_cast<const T *>(e->H->im32) : nullptr};
+    } else {
+        a.H = CsrView<T>{e->H->ptr, e->H->idx, reinterpret_cast<const T *>(e->H->re64),
+                         e->H->complex_values ? reinterpret_cast<const T *>(e->H->im64) : nullptr};
+    }
+    const double hw = length > 1 ? half : 1.;  // a single moment never applies the operator
+    a.center = center;
+    a.half = hw;
+    a.inv_half = (T)(1. / hw);
+    a.partial = partial;
+    a.ticket = ticket;
+    a.mu = mu;
+    a.mlen = length;
+    a.bcols = (int)b;
+    const V *t0;
+    if (C == 2) {
+        const int64_t total = n * U;
+        const int eg = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, (int64_t)sm_count() * 16));
+        to_f32_kernel<<<eg, 256, 0, s>>>(B, reinterpret_cast<float4 *>(tb), n, (int)b, U);
+        count_launch();
+        if (need_bra) {
+            to_f32_kernel<<<eg, 256, 0, s>>>(B, reinterpret_cast<float4 *>(bra), n, (int)b, U);
+            count_launch();
+        }
+        t0 = tb;
+        a.bra = bra;
+    } else {
+        t0 = reinterpret_cast<const V *>(B);
+        a.bra = reinterpret_cast<const V *>(B);
+    }
+    // Step 1 (always in the product form): mu_0 = <T0,T0>, mu_1 = <T0,T1>.
+    // Then T_k over two rotating buffers; in FP64 the read-only input is T0.
+    const int64_t steps = length == 1 ? 1 : doubling ? (length + 1) / 2 : length - 1;
+    const V *curr = t0, *prev = nullptr;
+    V *spare = ta, *second = C == 2 ? nullptr : tb;
+    for (int64_t k = 1; k <= steps; ++k) {
+        V *next = k == 1 ? spare : (k == 2 && second != nullptr) ? second : const_cast<V *>(prev);
+        a.curr = curr;
+        a.prev = prev;
+        a.next = next;
+        a.first = k == 1;
+        if (k == 1 || doubling) {
+            a.kmom = k - 1;
+            cheb_step_kernel<T, MU, MODE_DOUBLING, true, false><<<g_first, kThreads, smem, s>>>(a);
+        } else {
+            a.kmom = k;
+            cheb_step_kernel<T, MU, MODE_DIRECT, true, false><<<g_rest, kThreads, smem, s>>>(a);
+        }
+        count_launch();
+        prev = curr;
+        curr = next;
+    }
+    e->h_calls += length > 1 ? steps : 0;
+    KMSD_CUDA(cudaGetLastError());
+    return KMSD_OK;
+}
+
+template <class T>
+int dispatch(kmsd_engine_s *e, const double2 *B, double *mu, int64_t b, int64_t length, double center, double half,
+             bool doubling, cudaStream_t s) {
+    constexpr int C = Unit<T>::C;
+    const RowMap mp = make_map((int)((b + C - 1) / C), kThreads);
+    switch (mu_for(mp)) {
+        case 1: return run<T, 1>(e, B, mu, b, length, center, half, doubling, s);
+        case 2: return run<T, 2>(e, B, mu, b, length, center, half, doubling, s);
+        case 4: return run<T, 4>(e, B, mu, b, length, center, half, doubling, s);
+        case 8: return run<T, 8>(e, B, mu, b, length, center, half, doubling, s);
+    }
+    return fail(KMSD_EINVAL, "too many columns for one engine call");
+}
+
+}  // namespace
+
+extern "C" int kmsd_engine_moments_noalloc(kmsd_engine e, const void *b_in, double *mu, int64_t b, int64_t length,
+                                           double center, double half, int flags, void *stream) {
+    if (!e || !e->H || !b_in || !mu || b < 1) return fail(KMSD_EINVAL, "expected nonempty finite (N,batch) array");
+    if (length < 1) return fail(KMSD_EINVAL, "moment count must be positive");
+    if (length > 1 && !(half > 0)) return fail(KMSD_EINVAL, "spectral half-width must be positive");
+    if (!e->identity)
+        return fail(KMSD_EINVAL, "kmsd_engine_moments_noalloc supports orthogonal-basis engines (S = I) only");
+    const bool doubling = (flags & KMSD_MOMENTS_DOUBLING) != 0;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const double2 *B = static_cast<const double2 *>(b_in);
+    if (e->precision == KMSD_MIXED) {
+        if (e->H->re32 == nullptr)
+            return fail(KMSD_EINVAL, "kmsd_engine_moments_noalloc: the mixed-precision engine has no complex64 copy "
+                                     "of H yet; one allocating call (kmsd_engine_moments) creates it");
+        return dispatch<float>(e, B, mu, b, length, center, half, doubling, s);
+    }
+    return dispatch<double>(e, B, mu, b, length, center, half, doubling, s);
+}

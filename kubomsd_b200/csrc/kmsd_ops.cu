@@ -18,24 +18,6 @@
 
 using namespace kmsd;
 
-struct kmsd_engine_s {
-    kmsd_csr_s *H = nullptr;
-    kmsd_metric_s *M = nullptr;
-    int vel_kind[3] = {-1, -1, -1};
-    kmsd_csr_s *vel[9] = {};
-    double rtol = 1e-10, atol = 0., hbar = 0.6582119569509067;
-    int maxiter = 1000;
-    int precision = KMSD_FP64;
-    int64_t h_calls = 0, v_calls = 0;
-    bool identity = false;
-    DevBuf ta, tb, bra, hx, t1, t2, t3, t4, t5, psi, vc, inj[3], outw;
-    DevBuf status;  // int[4]: [0] code, [1] report claim, [2] series nonfinite
-    DevBuf report;  // FailReportFull
-    DevBuf dots;    // double2[512]
-    Reducer red;
-    FailReportFull last{};
-};
-
 namespace {
 using E = kmsd_engine_s;
 
