@@ -7,12 +7,13 @@ BackendUnavailable with the build command.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import re
 from pathlib import Path
 
 from .errors import BackendUnavailable
 
-LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libkmsd_b200.so"
+LIB_PATH = Path(os.environ.get("KUBOMSD_B200_LIB", Path(__file__).resolve().parent / "_lib" / "libkmsd_b200.so"))
 HEADER = Path(__file__).resolve().parent.parent / "include" / "kmsd.h"
 
 KMSD_OK, KMSD_EINVAL, KMSD_ERUNTIME, KMSD_EMETRIC, KMSD_ECUDA = 0, 1, 2, 3, 4

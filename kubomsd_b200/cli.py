@@ -79,6 +79,8 @@ def parser():
     run.add_argument("--efermi-source")
     run.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     run.add_argument("--moment-doubling", action="store_true")
+    run.add_argument("--spectral-bounds-method", choices=["arpack", "device-lanczos"], default="arpack",
+                     help="host ARPACK (the reference's estimate) or Lanczos on the device")
     sub.add_parser("capabilities", help="report the B200 backend's availability")
     return p
 
@@ -129,6 +131,7 @@ def _config(args):
                      integration_dt_fs=args.integration_dt_fs, include_vac=not args.no_vac, rho_abs=args.rho_abs,
                      rho_rel=args.rho_rel, memory_limit_gb=args.memory_limit_gb, precision=args.precision,
                      moment_doubling=args.moment_doubling, output_npz=args.npz,
+                     bounds_method=args.spectral_bounds_method,
                      transport_distribution=args.transport_distribution)
 
 

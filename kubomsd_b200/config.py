@@ -91,6 +91,7 @@ class RunConfig:
     rho_rel: float = 1e-12
     memory_limit_gb: float = 4.
     output_npz: bool = False
+    bounds_method: str = "arpack"
     precision: str = "fp64"
     moment_doubling: bool = False
 
@@ -129,6 +130,8 @@ class RunConfig:
             raise KuboMSDError("metric_gap_ratio must be strictly between zero and one")
         if self.precision not in ("fp64", "mixed"):
             raise KuboMSDError("precision must be fp64 or mixed")
+        if self.bounds_method not in ("arpack", "device-lanczos"):
+            raise KuboMSDError("bounds_method must be arpack or device-lanczos")
         if self.spectral_bounds is not None:
             b = tuple(float(v) for v in self.spectral_bounds)
             if len(b) != 2 or not np.isfinite(b).all() or b[0] >= b[1]:

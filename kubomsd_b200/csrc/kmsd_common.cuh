@@ -79,6 +79,16 @@ template <class T> struct CsrView {
     const T *im;  // nullptr for a real matrix
 };
 
+// The same matrix as a row-major ELL block [n][w] (w a multiple of 4; short
+// rows padded with zero values pointing at their own row), so a row's
+// indices and values are 16-byte vector loads and no row pointer is read.
+template <class T> struct EllView {
+    const int *idx;
+    const T *re;
+    const T *im;  // nullptr for a real matrix
+    int w;        // 0: no ELL form
+};
+
 // ---------------------------------------------------------------- mapping
 struct RowMap {
     int G;      // threads per row group (power of two, <= 32)

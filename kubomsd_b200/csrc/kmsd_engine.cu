@@ -133,6 +133,21 @@ int kmsd_csr_s::ensure_f32() {
         KMSD_CUDA(cudaMalloc(&im32, std::max<int64_t>(nnz, 1) * sizeof(float)));
         KMSD_CUDA(cudaMemcpy(im32, f.data(), nnz * sizeof(float), cudaMemcpyHostToDevice));
     }
+    if (ell_w > 0) {
+        const int64_t m = n * ell_w;
+        std::vector<double> he(m);
+        std::vector<float> fe(m);
+        KMSD_CUDA(cudaMemcpy(he.data(), ell_re64, m * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < m; ++i) fe[i] = (float)he[i];
+        KMSD_CUDA(cudaMalloc(&ell_re32, m * sizeof(float)));
+        KMSD_CUDA(cudaMemcpy(ell_re32, fe.data(), m * sizeof(float), cudaMemcpyHostToDevice));
+        if (complex_values) {
+            KMSD_CUDA(cudaMemcpy(he.data(), ell_im64, m * sizeof(double), cudaMemcpyDeviceToHost));
+            for (int64_t i = 0; i < m; ++i) fe[i] = (float)he[i];
+            KMSD_CUDA(cudaMalloc(&ell_im32, m * sizeof(float)));
+            KMSD_CUDA(cudaMemcpy(ell_im32, fe.data(), m * sizeof(float), cudaMemcpyHostToDevice));
+        }
+    }
     return KMSD_OK;
 }
 
@@ -327,6 +342,29 @@ int kmsd_csr_create(int64_t n, const int64_t *indptr, const int64_t *indices, co
     if (!rc) rc = up((void **)&A->idx, i32.data(), nnz * sizeof(int));
     if (!rc) rc = up((void **)&A->re64, val_re, nnz * sizeof(double));
     if (!rc && cplx) rc = up((void **)&A->im64, val_im, nnz * sizeof(double));
+    // ELL form when rows are short and padding costs at most a quarter of the
+    // index/value bytes (lattice Hamiltonians: every row has the same length).
+    int64_t lmax = 0;
+    for (int64_t r = 0; r < n; ++r) lmax = std::max<int64_t>(lmax, indptr[r + 1] - indptr[r]);
+    const int64_t w = std::max<int64_t>(4, (lmax + 3) / 4 * 4);
+    if (!rc && lmax > 0 && w <= 32 && n * w <= nnz + nnz / 4 + 4) {
+        const int64_t m = n * w;
+        std::vector<int> ei(m);
+        std::vector<double> er(m, 0.), eim(cplx ? m : 0, 0.);
+        for (int64_t r = 0; r < n; ++r) {
+            int64_t j = 0;
+            for (int64_t k = indptr[r]; k < indptr[r + 1]; ++k, ++j) {
+                ei[r * w + j] = (int)indices[k];
+                er[r * w + j] = val_re[k];
+                if (cplx) eim[r * w + j] = val_im[k];
+            }
+            for (; j < w; ++j) ei[r * w + j] = (int)r;  // zero-valued padding on the own row
+        }
+        rc = up((void **)&A->ell_idx, ei.data(), m * sizeof(int));
+        if (!rc) rc = up((void **)&A->ell_re64, er.data(), m * sizeof(double));
+        if (!rc && cplx) rc = up((void **)&A->ell_im64, eim.data(), m * sizeof(double));
+        if (!rc) A->ell_w = (int)w;
+    }
     if (rc) {
         kmsd_csr_destroy(A);
         return rc;
@@ -343,6 +381,11 @@ void kmsd_csr_destroy(kmsd_csr a) {
     cudaFree(a->im64);
     cudaFree(a->re32);
     cudaFree(a->im32);
+    cudaFree(a->ell_idx);
+    cudaFree(a->ell_re64);
+    cudaFree(a->ell_im64);
+    cudaFree(a->ell_re32);
+    cudaFree(a->ell_im32);
     delete a;
 }
 

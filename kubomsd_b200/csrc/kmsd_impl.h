@@ -56,9 +56,16 @@ struct kmsd_csr_s {
     bool complex_values = false;
     bool identity = false;
     int device = 0;
+    // ELL copy for short rows (see EllView); ell_w == 0 when not built.
+    int ell_w = 0;
+    int *ell_idx = nullptr;
+    double *ell_re64 = nullptr, *ell_im64 = nullptr;
+    float *ell_re32 = nullptr, *ell_im32 = nullptr;
     int ensure_f32();
     kmsd::CsrView<double> view64() const { return {ptr, idx, re64, complex_values ? im64 : nullptr}; }
     kmsd::CsrView<float> view32() const { return {ptr, idx, re32, complex_values ? im32 : nullptr}; }
+    kmsd::EllView<double> ell64() const { return {ell_idx, ell_re64, complex_values ? ell_im64 : nullptr, ell_w}; }
+    kmsd::EllView<float> ell32() const { return {ell_idx, ell_re32, complex_values ? ell_im32 : nullptr, ell_w}; }
 };
 
 namespace kmsd {

@@ -61,6 +61,49 @@ __device__ __forceinline__ void gather_row(const CsrView<T> &A, const typename U
     }
 }
 
+// Four matrix values starting at a 16-byte aligned element.
+__device__ __forceinline__ void ld4(const float *p, float (&v)[4]) {
+    const float4 q = __ldg(reinterpret_cast<const float4 *>(p));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void ld4(const double *p, double (&v)[4]) {
+    const double2 q0 = __ldg(reinterpret_cast<const double2 *>(p));
+    const double2 q1 = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+    v[0] = q0.x; v[1] = q0.y; v[2] = q1.x; v[3] = q1.y;
+}
+
+// acc[m] += sum_k A[row,k] X[k, unit u_m] over the ELL row: one int4 of
+// column indices and one 16-byte load of values per four entries, all four
+// gathers of a chunk issued before their multiply-adds.
+template <class T, int MU>
+__device__ __forceinline__ void gather_row_ell(const EllView<T> &A, const typename Unit<T>::vec *X, int64_t row,
+                                               int U, int G, int lane, Pk<T> (&acc)[MU]) {
+    const int4 *ip = reinterpret_cast<const int4 *>(A.idx + row * A.w);
+    const T *rp = A.re + row * A.w;
+    const T *jp = A.im ? A.im + row * A.w : nullptr;
+    for (int k4 = 0; k4 < A.w / 4; ++k4) {
+        const int4 c = __ldg(ip + k4);
+        T vr[4], vi[4];
+        ld4(rp + 4 * k4, vr);
+        if (jp) ld4(jp + 4 * k4, vi);
+        const int col[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+        for (int m = 0; m < MU; ++m) {
+            const int u = lane + m * G;
+            if (u < U) {
+                Pk<T> xs[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) xs[j] = ldg(X + (size_t)col[j] * U + u);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (jp) cmac_cplx(acc[m], vr[j], vi[j], xs[j]);
+                    else cmac_real(acc[m], vr[j], xs[j]);
+                }
+            }
+        }
+    }
+}
+
 // Same for one unit (runtime loop callers).
 template <class T>
 __device__ __forceinline__ Pk<T> gather_unit(const CsrView<T> &A, const typename Unit<T>::vec *X,
@@ -140,6 +183,7 @@ template <class T> struct StepArgs {
     int64_t n;
     RowMap mp;
     CsrView<T> H;          // inline operator (identity metric)
+    EllView<T> E;          // the same operator in ELL form (HSRC_ELL)
     const V *hx;           // precomputed S^-1 H x (general metric), or nullptr
     const V *curr;         // T_{k-1} (= x)
     const V *prev;         // T_{k-2}; may alias `next`
@@ -173,8 +217,56 @@ template <class T> struct StepArgs {
     int *status;           // nonfinite flag for series output
 };
 
-template <class T, int MU, int MODE, bool INLINE_H, bool INLINE_V>
-__global__ void __launch_bounds__(256) cheb_step_kernel(const StepArgs<T> a) {
+// Where h = S^-1 H x comes from: a solved operand (general metric), CSR,
+// ELL of any width, or real ELL of width 4 / 8 whose next row's indices and
+// values are prefetched one grid-stride iteration ahead, so each row waits on
+// one memory latency (its gathers) instead of three.
+enum { HSRC_SOLVED = 0, HSRC_CSR = 1, HSRC_ELL = 2, HSRC_ELL4 = 3, HSRC_ELL8 = 4 };
+
+// Minimum resident CTAs per SM asked of the compiler for the one-unit-per-lane
+// step kernels.  The kernel is latency bound; on B200 four CTAs of 256
+// threads (<= 64 registers) measured best for the moment steps.
+#ifndef KMSD_STEP_MINB
+#define KMSD_STEP_MINB 4
+#endif
+
+template <class T, int PF> struct EllRow {
+    int4 idx[PF];
+    T val[PF][4];
+};
+template <class T, int PF>
+__device__ __forceinline__ void ell_row_load(const EllView<T> &A, int64_t row, EllRow<T, PF> &r) {
+    const int4 *ip = reinterpret_cast<const int4 *>(A.idx + row * (4 * PF));
+    const T *vp = A.re + row * (4 * PF);
+#pragma unroll
+    for (int q = 0; q < PF; ++q) {
+        r.idx[q] = __ldg(ip + q);
+        ld4(vp + 4 * q, r.val[q]);
+    }
+}
+// acc[m] += sum over the prefetched ELL row (real values).
+template <class T, int MU, int PF>
+__device__ __forceinline__ void gather_prefetched(const EllRow<T, PF> &r, const typename Unit<T>::vec *X, int U,
+                                                  int G, int lane, Pk<T> (&acc)[MU]) {
+#pragma unroll
+    for (int m = 0; m < MU; ++m) {
+        const int u = lane + m * G;
+        if (u < U) {
+#pragma unroll
+            for (int q = 0; q < PF; ++q) {
+                const int col[4] = {r.idx[q].x, r.idx[q].y, r.idx[q].z, r.idx[q].w};
+                Pk<T> xs[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) xs[j] = ldg(X + (size_t)col[j] * U + u);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) cmac_real(acc[m], r.val[q][j], xs[j]);
+            }
+        }
+    }
+}
+
+template <class T, int MU, int MODE, int HSRC, bool INLINE_V>
+__global__ void __launch_bounds__(256, (MU == 1 ? KMSD_STEP_MINB : 1)) cheb_step_kernel(const StepArgs<T> a) {
     using V = typename Unit<T>::vec;
     constexpr int C = Unit<T>::C;
     extern __shared__ double2 smem[];
@@ -190,20 +282,43 @@ __global__ void __launch_bounds__(256) cheb_step_kernel(const StepArgs<T> a) {
         }
     const T cen = (T)a.center, hal = (T)a.half;
     bool bad = false;
-    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < a.n; row += (int64_t)gridDim.x * mp.gpc) {
+    constexpr int PF = HSRC == HSRC_ELL4 ? 1 : HSRC == HSRC_ELL8 ? 2 : 1;
+    const int64_t stride = (int64_t)gridDim.x * mp.gpc;
+    EllRow<T, PF> ahead;
+    if ((HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8) && (int64_t)blockIdx.x * mp.gpc + g < a.n)
+        ell_row_load<T, PF>(a.E, (int64_t)blockIdx.x * mp.gpc + g, ahead);
+    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < a.n; row += stride) {
+        EllRow<T, PF> cur;
+        if (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8) {
+            cur = ahead;
+            if (row + stride < a.n) ell_row_load<T, PF>(a.E, row + stride, ahead);
+        }
+        // Row-local operands first, so their latency overlaps the gathers.
+        Pk<T> xo[MU], po[MU];
+#pragma unroll
+        for (int m = 0; m < MU; ++m) {
+            const int u = lane + m * mp.G;
+            if (u < mp.U) {
+                const size_t o = (size_t)row * mp.U + u;
+                xo[m] = ld(a.curr + o);
+                po[m] = a.first ? pk_zero<T>() : ld(a.prev + o);
+            }
+        }
         Pk<T> h[MU];
-        if (INLINE_H) {
+        if (HSRC != HSRC_SOLVED) {
 #pragma unroll
             for (int m = 0; m < MU; ++m) h[m] = pk_zero<T>();
-            gather_row<T, MU>(a.H, a.curr, row, mp.U, mp.G, lane, h);
+            if (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8) gather_prefetched<T, MU, PF>(cur, a.curr, mp.U, mp.G, lane, h);
+            else if (HSRC == HSRC_ELL) gather_row_ell<T, MU>(a.E, a.curr, row, mp.U, mp.G, lane, h);
+            else gather_row<T, MU>(a.H, a.curr, row, mp.U, mp.G, lane, h);
         }
 #pragma unroll
         for (int m = 0; m < MU; ++m) {
             const int u = lane + m * mp.G;
             if (u >= mp.U) continue;
             const size_t o = (size_t)row * mp.U + u;
-            const Pk<T> x = ld(a.curr + o);
-            const Pk<T> hv = INLINE_H ? h[m] : ld(a.hx + o);
+            const Pk<T> x = xo[m];
+            const Pk<T> hv = HSRC != HSRC_SOLVED ? h[m] : ld(a.hx + o);
             Pk<T> t;
 #pragma unroll
             for (int c = 0; c < C; ++c) {
@@ -237,7 +352,7 @@ __global__ void __launch_bounds__(256) cheb_step_kernel(const StepArgs<T> a) {
             if (a.first) {
                 nx = t;
             } else {
-                const Pk<T> p = ld(a.prev + o);
+                const Pk<T> p = po[m];
 #pragma unroll
                 for (int c = 0; c < C; ++c) {
                     nx.re[c] = T(2) * t.re[c] - p.re[c];

@@ -115,37 +115,37 @@ __device__ __forceinline__ void precond(const Pre &P, int64_t bi, int64_t r0, in
             const double2 d = L[i * m + i];
             z[i] = cdiv(v, make_double2(d.x, -d.y));
         }
-        return;
-    }
+    } else {
 #pragma unroll
-    for (int i = 0; i < MAXB; ++i) {
-        if (i < m) {
-            double2 v = r[i];
+        for (int i = 0; i < MAXB; ++i) {
+            if (i < m) {
+                double2 v = r[i];
 #pragma unroll
-            for (int k = 0; k < MAXB; ++k) {
-                if (k < i) {
-                    const double2 l = L[i * m + k];
-                    v.x -= l.x * z[k].x - l.y * z[k].y;
-                    v.y -= l.x * z[k].y + l.y * z[k].x;
+                for (int k = 0; k < MAXB; ++k) {
+                    if (k < i) {
+                        const double2 l = L[i * m + k];
+                        v.x -= l.x * z[k].x - l.y * z[k].y;
+                        v.y -= l.x * z[k].y + l.y * z[k].x;
+                    }
                 }
+                z[i] = cdiv(v, L[i * m + i]);
             }
-            z[i] = cdiv(v, L[i * m + i]);
         }
-    }
 #pragma unroll
-    for (int i = MAXB - 1; i >= 0; --i) {
-        if (i < m) {
-            double2 v = z[i];
+        for (int i = MAXB - 1; i >= 0; --i) {
+            if (i < m) {
+                double2 v = z[i];
 #pragma unroll
-            for (int k = 0; k < MAXB; ++k) {
-                if (k > i && k < m) {
-                    const double2 l = L[k * m + i];  // conj(l) * z[k]
-                    v.x -= l.x * z[k].x + l.y * z[k].y;
-                    v.y -= l.x * z[k].y - l.y * z[k].x;
+                for (int k = 0; k < MAXB; ++k) {
+                    if (k > i && k < m) {
+                        const double2 l = L[k * m + i];  // conj(l) * z[k]
+                        v.x -= l.x * z[k].x + l.y * z[k].y;
+                        v.y -= l.x * z[k].y - l.y * z[k].x;
+                    }
                 }
+                const double2 d = L[i * m + i];
+                z[i] = cdiv(v, make_double2(d.x, -d.y));
             }
-            const double2 d = L[i * m + i];
-            z[i] = cdiv(v, make_double2(d.x, -d.y));
         }
     }
 }

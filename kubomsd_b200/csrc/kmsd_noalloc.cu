@@ -74,7 +74,7 @@ template <class T, int MU, int MODE>
 int occupancy_grid(int64_t n, const RowMap &mp, size_t smem, int *grid) {
     int per_sm = 0;
     KMSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, cheb_step_kernel<T, MU, MODE, true, false>, kThreads, smem));
+        &per_sm, cheb_step_kernel<T, MU, MODE, HSRC_CSR, false>, kThreads, smem));
     if (per_sm < 1) per_sm = 1;
     const int64_t need = (n + mp.gpc - 1) / mp.gpc;
     *grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sm_count() * per_sm));
@@ -168,10 +168,10 @@ int run(kmsd_engine_s *e, const double2 *B, double *mu, int64_t b, int64_t lengt
         a.first = k == 1;
         if (k == 1 || doubling) {
             a.kmom = k - 1;
-            cheb_step_kernel<T, MU, MODE_DOUBLING, true, false><<<g_first, kThreads, smem, s>>>(a);
+            cheb_step_kernel<T, MU, MODE_DOUBLING, HSRC_CSR, false><<<g_first, kThreads, smem, s>>>(a);
         } else {
             a.kmom = k;
-            cheb_step_kernel<T, MU, MODE_DIRECT, true, false><<<g_rest, kThreads, smem, s>>>(a);
+            cheb_step_kernel<T, MU, MODE_DIRECT, HSRC_CSR, false><<<g_rest, kThreads, smem, s>>>(a);
         }
         count_launch();
         prev = curr;

@@ -146,9 +146,9 @@ int v_cov(E *e, const double *dir, const double2 *B, double2 *out, int64_t b, co
 // this kernel (occupancy API), capped by the rows to cover.  Fixed per kernel
 // and shape, so row ownership — and with it every reduction order — is
 // reproducible run to run.
-template <class T, int MU, int MODE, bool IH, bool IV>
+template <class T, int MU, int MODE, int HSRC, bool IV>
 int launch_step_mu(E *e, StepArgs<T> &a, cudaStream_t s) {
-    const auto kern = cheb_step_kernel<T, MU, MODE, IH, IV>;
+    const auto kern = cheb_step_kernel<T, MU, MODE, HSRC, IV>;
     const size_t sm = reduce_smem(a.mp, Unit<T>::C);
     const int grid = wave_grid((const void *)kern, sm, a.n, a.mp);
     if (MODE == MODE_DIRECT || MODE == MODE_DOUBLING) {
@@ -160,16 +160,28 @@ int launch_step_mu(E *e, StepArgs<T> &a, cudaStream_t s) {
     return KMSD_OK;
 }
 
+template <class T, int MODE, int HSRC, bool IV>
+int launch_step_h(E *e, StepArgs<T> &a, cudaStream_t s) {
+    switch (mu_for(a.mp)) {
+        case 1: return launch_step_mu<T, 1, MODE, HSRC, IV>(e, a, s);
+        case 2: return launch_step_mu<T, 2, MODE, HSRC, IV>(e, a, s);
+        case 4: return launch_step_mu<T, 4, MODE, HSRC, IV>(e, a, s);
+        case 8: return launch_step_mu<T, 8, MODE, HSRC, IV>(e, a, s);
+    }
+    return fail(KMSD_EINVAL, "too many columns for one engine call");
+}
+
+// IH: the operator is applied inline (identity metric), from the ELL form
+// when the matrix has one, else from CSR; otherwise the step reads the solved
+// operand a.hx.
 template <class T, int MODE, bool IH, bool IV>
 int launch_step(E *e, StepArgs<T> &a, cudaStream_t s) {
     int rc;
-    switch (mu_for(a.mp)) {
-        case 1: rc = launch_step_mu<T, 1, MODE, IH, IV>(e, a, s); break;
-        case 2: rc = launch_step_mu<T, 2, MODE, IH, IV>(e, a, s); break;
-        case 4: rc = launch_step_mu<T, 4, MODE, IH, IV>(e, a, s); break;
-        case 8: rc = launch_step_mu<T, 8, MODE, IH, IV>(e, a, s); break;
-        default: return fail(KMSD_EINVAL, "too many columns for one engine call");
-    }
+    if (!IH) rc = launch_step_h<T, MODE, HSRC_SOLVED, IV>(e, a, s);
+    else if (a.E.w == 4 && a.E.im == nullptr) rc = launch_step_h<T, MODE, HSRC_ELL4, IV>(e, a, s);
+    else if (a.E.w == 8 && a.E.im == nullptr) rc = launch_step_h<T, MODE, HSRC_ELL8, IV>(e, a, s);
+    else if (a.E.w > 0) rc = launch_step_h<T, MODE, HSRC_ELL, IV>(e, a, s);
+    else rc = launch_step_h<T, MODE, HSRC_CSR, IV>(e, a, s);
     if (rc) return rc;
     count_launch();
     KMSD_CUDA(cudaGetLastError());
@@ -179,6 +191,13 @@ int launch_step(E *e, StepArgs<T> &a, cudaStream_t s) {
 template <class T> CsrView<T> view_of(kmsd_csr_s *A);
 template <> CsrView<double> view_of<double>(kmsd_csr_s *A) { return A->view64(); }
 template <> CsrView<float> view_of<float>(kmsd_csr_s *A) { return A->view32(); }
+template <class T> EllView<T> ell_of(kmsd_csr_s *A);
+template <> EllView<double> ell_of<double>(kmsd_csr_s *A) { return A->ell64(); }
+template <> EllView<float> ell_of<float>(kmsd_csr_s *A) {
+    EllView<float> v = A->ell32();
+    if (v.re == nullptr) v.w = 0;  // no complex64 ELL values yet: use CSR
+    return v;
+}
 
 template <class T> StepArgs<T> base_args(E *e, int U, double center, double half) {
     StepArgs<T> a;
@@ -186,6 +205,7 @@ template <class T> StepArgs<T> base_args(E *e, int U, double center, double half
     a.n = e->H->n;
     a.mp = make_map(U, kThreads);
     a.H = view_of<T>(e->H);
+    a.E = ell_of<T>(e->H);
     a.center = center;
     a.half = half;
     a.inv_half = (T)(1. / half);

@@ -261,8 +261,11 @@ def iter_stochastic_blocks(ops, config, method="stepwise", samples=None, paralle
     ctx = parallel or ParallelContext()
     cfg = config
     if bounds_report is None:
-        bounds_report = ctx.root_call("spectral bounds", lambda: kpm.estimate_spectral_bounds(
-            ops.host_H, ops.host_S, ops.metric.s_lower, cfg))
+        if getattr(cfg, "bounds_method", "arpack") == "device-lanczos":
+            bounds_report = kpm.lanczos_spectral_bounds(ops, cfg)
+        else:
+            bounds_report = ctx.root_call("spectral bounds", lambda: kpm.estimate_spectral_bounds(
+                ops.host_H, ops.host_S, ops.metric.s_lower, cfg))
     cfg = replace(cfg, spectral_bounds=bounds_report["bounds"])
     ns = cfg.nsamples if samples is None else samples.shape[1]
     nbk = (ns + cfg.statistics_block - 1) // cfg.statistics_block
