@@ -101,10 +101,12 @@ inline int next_pow2(int x) {
     while (p < x) p <<= 1;
     return p;
 }
+// Row groups span up to four warps (G <= 128), so rows of up to 128 units
+// keep one unit per lane; wider rows give each lane several units.
 inline RowMap make_map(int U, int threads) {
     RowMap m;
     m.U = U;
-    m.G = U >= 32 ? 32 : next_pow2(U < 1 ? 1 : U);
+    m.G = U >= 128 ? 128 : next_pow2(U < 1 ? 1 : U);
     m.gpc = threads / m.G;
     return m;
 }

@@ -97,6 +97,9 @@ int wave_grid(const void *kernel, size_t smem, int64_t rows, const RowMap &mp) {
     return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sm_count() * per_sm));
 }
 int mu_for(const RowMap &mp) {
+    // At most 256 units (512 reduction columns) per launch: the fixed-size
+    // shared buffers of the reductions are sized for that.
+    if (mp.U > 256) return 0;
     const int per = (mp.U + mp.G - 1) / mp.G;
     if (per <= 1) return 1;
     if (per <= 2) return 2;

@@ -266,7 +266,8 @@ __device__ __forceinline__ void gather_prefetched(const EllRow<T, PF> &r, const 
 }
 
 template <class T, int MU, int MODE, int HSRC, bool INLINE_V>
-__global__ void __launch_bounds__(256, (MU == 1 ? KMSD_STEP_MINB : 1)) cheb_step_kernel(const StepArgs<T> a) {
+__global__ void __launch_bounds__(256, (MU == 1 && MODE != MODE_SERIES ? KMSD_STEP_MINB : 1))
+    cheb_step_kernel(const StepArgs<T> a) {
     using V = typename Unit<T>::vec;
     constexpr int C = Unit<T>::C;
     extern __shared__ double2 smem[];

@@ -228,6 +228,47 @@ class B200Metric:
             rc = self.lib.kmsd_metric_create(self.S.handle, _dptr(diag), 0, None, None, None, None, C.byref(handle))
         _check(self.lib, rc)
         self.handle = handle
+        self._create = (diag, blocks, config)
+        self.policy = (getattr(config, "metric_residual_policy", "fixed"), getattr(config, "metric_check_interval", 32),
+                       getattr(config, "metric_gap_ratio", .1))
+        self._set_policy(*self.policy)
+        self.identity = bool(self.lib.kmsd_metric_is_identity(handle))
+
+    def replica(self):
+        """A second metric over the same uploaded S with its own workspace, for
+        concurrent use from another stream (handles are one-call-at-a-time)."""
+        diag, blocks, config = self._create
+        other = object.__new__(B200Metric)
+        other.lib = self.lib
+        other.S = self.S
+        other.n = self.n
+        B200Metric._init_handle(other, diag, blocks, config)
+        return other
+
+    def _init_handle(self, diag, blocks, config):
+        handle = C.c_void_p()
+        nblocks = len(blocks)
+        if nblocks:
+            start = np.zeros(nblocks + 1, np.int64)
+            offs = np.zeros(nblocks, np.int64)
+            facs, pos = [], 0
+            for i, (a, b, L) in enumerate(blocks):
+                L = np.asarray(L, dtype=np.complex128)
+                start[i], start[i + 1] = a, b
+                offs[i] = pos
+                facs.append(L.ravel())
+                pos += L.size
+            fac = np.concatenate(facs)
+            fre, fim = np.ascontiguousarray(fac.real), np.ascontiguousarray(fac.imag)
+            rc = self.lib.kmsd_metric_create(self.S.handle, _dptr(diag), nblocks,
+                                             start.ctypes.data_as(C.POINTER(C.c_int64)),
+                                             offs.ctypes.data_as(C.POINTER(C.c_int64)), _dptr(fre), _dptr(fim),
+                                             C.byref(handle))
+        else:
+            rc = self.lib.kmsd_metric_create(self.S.handle, _dptr(diag), 0, None, None, None, None, C.byref(handle))
+        _check(self.lib, rc)
+        self.handle = handle
+        self._create = (diag, blocks, config)
         self.policy = (getattr(config, "metric_residual_policy", "fixed"), getattr(config, "metric_check_interval", 32),
                        getattr(config, "metric_gap_ratio", .1))
         self._set_policy(*self.policy)
@@ -359,14 +400,29 @@ class B200Operators:
                 d = DeviceCSR(m, self.lib)
                 self._keep.append(d)
                 mats[3 * ai + j] = d.handle
+        self._kinds, self._mats, self._config = kinds, mats, config
+        self._create_engine()
+
+    def _create_engine(self):
         handle = C.c_void_p()
-        rc = self.lib.kmsd_engine_create(self.H.handle, metric.handle, kinds, mats, float(config.metric_rtol),
-                                         float(config.metric_atol), int(config.metric_maxiter), HBAR_EV_FS,
-                                         _abi.KMSD_MIXED if self.precision == "mixed" else _abi.KMSD_FP64,
+        cfg = self._config
+        rc = self.lib.kmsd_engine_create(self.H.handle, self.metric.handle, self._kinds, self._mats,
+                                         float(cfg.metric_rtol), float(cfg.metric_atol), int(cfg.metric_maxiter),
+                                         HBAR_EV_FS, _abi.KMSD_MIXED if self.precision == "mixed" else _abi.KMSD_FP64,
                                          C.byref(handle))
         _check(self.lib, rc)
         self.handle = handle
         self.core = _Counters(self)
+
+    def replica(self):
+        """Another engine over the same uploaded H, S and velocity matrices with
+        its own metric and workspace: a handle serves one call at a time, so
+        concurrent streams each use their own replica."""
+        other = object.__new__(B200Operators)
+        other.__dict__.update({k: v for k, v in self.__dict__.items() if k not in ("handle", "core", "metric")})
+        other.metric = self.metric.replica()
+        other._create_engine()
+        return other
 
     # -- helpers
     def _counters(self):
