@@ -235,9 +235,9 @@ def run_serving(args):
     models = {
         "sq128": ResidentModel("sq128", lattices.square_lattice(128, seed=1), (-11.5, 11.5), precision="mixed",
                                replicas=8),
-        "hc1024": ResidentModel("hc1024", lattices.honeycomb(1024, 512, seed=2, with_velocity=False), (-9.2, 9.2),
+        "hc1024": ResidentModel("hc1024", lattices.honeycomb(1024, 512, seed=2), (-9.2, 9.2),
                                 precision="mixed", replicas=8),
-        "hc2048": ResidentModel("hc2048", lattices.honeycomb(2048, 1024, seed=3, with_velocity=False),
+        "hc2048": ResidentModel("hc2048", lattices.honeycomb(2048, 1024, seed=3),
                                 (-9.2, 9.2), precision="mixed", replicas=8),
         "sp3_2k": ResidentModel("sp3_2k", lattices.diamond_sp3(cells=4), (-40., 40.), precision="fp64",
                                 replicas=8),

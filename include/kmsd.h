@@ -258,6 +258,40 @@ int kmsd_engine_inner(kmsd_engine e, const void *a, const void *b_in, void *out,
 int kmsd_column_dot(const void *x, const void *y, int64_t n, int64_t b,
                     void *out, void *stream);
 
+/* ---- Ragged batches (the batching form; no counterpart in the reference) */
+
+/* A batch of `ninst` independent orthogonal-basis Hamiltonians of any sizes,
+ * concatenated block-diagonally and cut into row tiles of `tile_rows` rows
+ * (0: 2048) that never cross an instance.  The reference runs independent
+ * disorder realisations one after another (src/kubo_msd/solvers/stochastic.py
+ * per statistics block); here one kernel per Chebyshev step covers all
+ * instances.  precision: KMSD_FP64 or KMSD_MIXED. */
+typedef struct kmsd_batch_s *kmsd_batch;
+int kmsd_batch_create(int64_t ninst, const kmsd_csr *h, int precision,
+                      int64_t tile_rows, kmsd_batch *out);
+void kmsd_batch_destroy(kmsd_batch bt);
+
+/* Row offsets of the instances in the concatenated vector block (ninst+1
+ * values, host). */
+int kmsd_batch_rows(kmsd_batch bt, int64_t *offsets);
+
+/* mu[(i*length + k)*b + j] = moment k of column j of instance i, the moments
+ * of kmsd_engine_moments for each instance with its own window
+ * (center[i], half[i]; host arrays).  b_in: the concatenated (sum N_i, b)
+ * complex128 block (device); mu: (ninst, length, b) float64 (device).
+ * use_graph = 1: the whole sequence of step and reduction kernels is
+ * captured once into a CUDA graph per (buffers, shape) and replayed.
+ * Synchronises the stream at the end. */
+int kmsd_batch_moments(kmsd_batch bt, const void *b_in, double *mu, int64_t b,
+                       int64_t length, const double *center, const double *half,
+                       int flags, int use_graph, void *stream);
+
+/* Autotuner: times the tile sizes 512..8192 rows on this call's shape and
+ * keeps the fastest (written to *chosen_tile_rows). */
+int kmsd_batch_tune(kmsd_batch bt, const void *b_in, double *mu, int64_t b,
+                    int64_t length, const double *center, const double *half,
+                    int flags, int64_t *chosen_tile_rows, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -70,6 +70,11 @@ SIGNATURES = {
     "kmsd_engine_failure_report": (C.c_int, [P, C.POINTER(SolveReport), I64, PI64]),
     "kmsd_engine_inner": (C.c_int, [P, P, P, P, I64, P]),
     "kmsd_column_dot": (C.c_int, [P, P, I64, I64, P, P]),
+    "kmsd_batch_create": (C.c_int, [I64, C.POINTER(P), C.c_int, I64, C.POINTER(P)]),
+    "kmsd_batch_destroy": (None, [P]),
+    "kmsd_batch_rows": (C.c_int, [P, PI64]),
+    "kmsd_batch_moments": (C.c_int, [P, P, PD, I64, I64, PD, PD, C.c_int, C.c_int, P]),
+    "kmsd_batch_tune": (C.c_int, [P, P, PD, I64, I64, PD, PD, C.c_int, PI64, P]),
 }
 
 

@@ -1,0 +1,90 @@
+"""Ragged batches of independent Hamiltonians (the batching form).
+
+`B200Batch` wraps `kmsd_batch_*` (include/kmsd.h): many orthogonal-basis
+Hamiltonians of uneven size, such as disorder realisations, concatenated
+block-diagonally on the device.  One kernel per Chebyshev step covers all of
+them, with per-instance spectral windows and per-instance moment reductions.
+The whole step sequence is captured into a CUDA graph and replayed.  `tune()`
+picks the row-tile size by timing.  The moments of every instance equal those
+of a separate `B200Operators.moments` call on it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from .native import DeviceCSR, _check, _ptr, _stream, _torch
+
+
+class B200Batch:
+    def __init__(self, hamiltonians, precision="mixed", tile_rows=0):
+        self.lib = _abi.require_library()
+        torch = _torch()
+        self.parts = [DeviceCSR(H, self.lib) for H in hamiltonians]
+        self.ninst = len(self.parts)
+        handles = (C.c_void_p * self.ninst)(*[p.handle.value for p in self.parts])
+        h = C.c_void_p()
+        rc = self.lib.kmsd_batch_create(self.ninst, handles, _abi.KMSD_MIXED if precision == "mixed" else
+                                        _abi.KMSD_FP64, int(tile_rows), C.byref(h))
+        _check(self.lib, rc)
+        self.handle = h
+        self.precision = precision
+        off = np.zeros(self.ninst + 1, np.int64)
+        _check(self.lib, self.lib.kmsd_batch_rows(h, off.ctypes.data_as(C.POINTER(C.c_int64))))
+        self.offsets = off
+        self.n = int(off[-1])
+        del torch
+
+    def concat(self, blocks):
+        """Concatenate per-instance (N_i, b) blocks into one device block."""
+        torch = _torch()
+        parts = [b if isinstance(b, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(b, np.complex128))
+                 for b in blocks]
+        return torch.cat([p.to("cuda", torch.complex128) for p in parts], dim=0).contiguous()
+
+    def moments(self, B, length, centers, halves, doubling=True, use_graph=True):
+        """(ninst, length, b) float64 device tensor of Jackson-KPM moments."""
+        torch = _torch()
+        if isinstance(B, (list, tuple)):
+            B = self.concat(B)
+        if B.shape[0] != self.n:
+            raise ValueError("batch block rows must equal the sum of instance sizes")
+        b = B.shape[1]
+        c = np.ascontiguousarray(np.broadcast_to(np.asarray(centers, float), (self.ninst,)))
+        h = np.ascontiguousarray(np.broadcast_to(np.asarray(halves, float), (self.ninst,)))
+        mu = getattr(self, "_mu", None)
+        if mu is None or mu.shape != (self.ninst, length, b):
+            mu = self._mu = torch.empty((self.ninst, length, b), dtype=torch.float64, device="cuda")
+        flags = _abi.KMSD_MOMENTS_DOUBLING if doubling else _abi.KMSD_MOMENTS_DIRECT
+        rc = self.lib.kmsd_batch_moments(self.handle, _ptr(B), C.cast(C.c_void_p(mu.data_ptr()),
+                                                                      C.POINTER(C.c_double)),
+                                         b, int(length), c.ctypes.data_as(C.POINTER(C.c_double)),
+                                         h.ctypes.data_as(C.POINTER(C.c_double)), flags, int(use_graph),
+                                         _stream(torch))
+        _check(self.lib, rc)
+        return mu.clone()
+
+    def tune(self, B, length, centers, halves, doubling=True):
+        torch = _torch()
+        if isinstance(B, (list, tuple)):
+            B = self.concat(B)
+        b = B.shape[1]
+        c = np.ascontiguousarray(np.broadcast_to(np.asarray(centers, float), (self.ninst,)))
+        h = np.ascontiguousarray(np.broadcast_to(np.asarray(halves, float), (self.ninst,)))
+        mu = torch.empty((self.ninst, length, b), dtype=torch.float64, device="cuda")
+        chosen = C.c_int64()
+        flags = _abi.KMSD_MOMENTS_DOUBLING if doubling else _abi.KMSD_MOMENTS_DIRECT
+        rc = self.lib.kmsd_batch_tune(self.handle, _ptr(B), C.cast(C.c_void_p(mu.data_ptr()), C.POINTER(C.c_double)),
+                                      b, int(length), c.ctypes.data_as(C.POINTER(C.c_double)),
+                                      h.ctypes.data_as(C.POINTER(C.c_double)), flags, C.byref(chosen),
+                                      _stream(torch))
+        _check(self.lib, rc)
+        return int(chosen.value)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            self.lib.kmsd_batch_destroy(h)
+            self.handle = None

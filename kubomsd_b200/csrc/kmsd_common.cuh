@@ -121,8 +121,36 @@ struct Ticket {
 };
 
 // Each thread holds `acc[m][c]` for its units u = lane + m*G (m < MU) and the
-// C columns of each unit.  Writes the CTA's per-column sums to
-// partial[blockIdx.x * ncol + col].  smem needs gpc * U * C double2.
+// C columns of each unit.  Writes the CTA's per-column sums to dst[col]
+// (the CTA's row of a partial-sum array).  smem needs gpc * U * C double2.
+template <int MU, int C>
+__device__ __forceinline__ void cta_column_sums_at(const double2 (&acc)[MU][C], const RowMap &mp,
+                                                   int ncol, double2 *smem, double2 *dst) {
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    if (g < mp.gpc) {
+#pragma unroll
+        for (int m = 0; m < MU; ++m) {
+            const int u = lane + m * mp.G;
+            if (u < mp.U) {
+#pragma unroll
+                for (int c = 0; c < C; ++c) smem[(g * mp.U + u) * C + c] = acc[m][c];
+            }
+        }
+    }
+    __syncthreads();
+    for (int col = threadIdx.x; col < ncol; col += blockDim.x) {
+        double sx = 0., sy = 0.;
+        for (int gg = 0; gg < mp.gpc; ++gg) {
+            const double2 v = smem[gg * mp.U * C + col];
+            sx += v.x;
+            sy += v.y;
+        }
+        dst[col] = make_double2(sx, sy);
+    }
+    __syncthreads();
+}
+
+// The same, written to partial[blockIdx.x * ncol + col].
 template <int MU, int C>
 __device__ __forceinline__ void cta_column_sums(const double2 (&acc)[MU][C], const RowMap &mp,
                                                 int ncol, double2 *smem, double2 *partial) {

@@ -538,7 +538,9 @@ class B200Operators:
         t, host = as_device(B, self.n)
         if length < 1:
             raise ValueError("moment count must be positive")
-        doubling = self.doubling if doubling is None else doubling
+        # the configured default applies the product identity where it holds (S = I);
+        # an explicit doubling=True on a nonorthogonal engine is an error
+        doubling = (self.doubling and self.metric.identity) if doubling is None else doubling
         flags = _abi.KMSD_MOMENTS_DOUBLING if doubling else _abi.KMSD_MOMENTS_DIRECT
         b = t.shape[1]
         mu = torch.empty((length, b), dtype=torch.float64, device=t.device)

@@ -1,0 +1,51 @@
+"""Ragged batch of independent Hamiltonians: one step kernel per Chebyshev
+step over all instances (captured in a CUDA graph) gives each instance the
+moments of a separate engine call."""
+import numpy as np
+import pytest
+
+from tests.helpers import assert_rel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def instances(cuda):
+    from kubomsd_b200 import kpm, lattices
+    rng = np.random.default_rng(4)
+    ms = []
+    for i, (lx, ly) in enumerate([(40, 20), (96, 48), (16, 8), (128, 64), (64, 32)]):
+        ms.append(lattices.honeycomb(lx, ly, W=float(rng.uniform(.1, 2.)), seed=100 + i, with_velocity=False))
+    ms.append(lattices.square_lattice(30, W=1.5, seed=7))  # different width: CSR path for the batch
+    blocks = [kpm.random_phases(m.n, 9 + i, range(16)) for i, m in enumerate(ms)]
+    bounds = [(-9.5, 9.5)] * 5 + [(-12., 12.)]
+    return ms, blocks, bounds
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("doubling", [False, True])
+def test_batch_moments_equal_separate_calls(instances, precision, doubling):
+    from kubomsd_b200.batch import B200Batch
+    from tests.gpu_util import engine
+    ms, blocks, bounds = instances
+    bt = B200Batch([m.H for m in ms], precision=precision, tile_rows=1024)
+    c = [(lo + hi) / 2 for lo, hi in bounds]
+    a = [(hi - lo) / 2 for lo, hi in bounds]
+    got = bt.moments(blocks, 96, c, a, doubling=doubling).cpu().numpy()
+    again = bt.moments(blocks, 96, c, a, doubling=doubling).cpu().numpy()  # graph replay
+    np.testing.assert_array_equal(got, again)
+    for i, m in enumerate(ms):
+        _, eng, _ = engine(m.H, m.S, precision=precision)
+        want = eng.moments(blocks[i], 96, c[i], a[i], doubling=doubling)
+        assert_rel(got[i], want, 1e-10, f"instance {i}")
+
+
+def test_batch_tuner_keeps_results(instances):
+    from kubomsd_b200.batch import B200Batch
+    ms, blocks, bounds = instances
+    bt = B200Batch([m.H for m in ms[:5]], precision="mixed")
+    c, a = [0.] * 5, [9.5] * 5
+    before = bt.moments(blocks[:5], 64, c, a).cpu().numpy()
+    rows = bt.tune(blocks[:5], 64, c, a)
+    assert rows in (512, 1024, 2048, 4096, 8192)
+    assert_rel(bt.moments(blocks[:5], 64, c, a).cpu().numpy(), before, 1e-12, "after tuning")

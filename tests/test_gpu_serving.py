@@ -30,7 +30,9 @@ def test_results_identical_alone_and_in_the_mix(models):
         kind = "msd" if i % 4 == 3 else "dos"
         reqs.append(Request(.01 * i, i, names[i % 3], kind, int(rng.choice([128, 256])), int(rng.choice([8, 16])),
                             1000 + i, [0., .5, 1.] if kind == "msd" else None))
-    mixed = Server(models, slots=4).serve(reqs)
+    srv = Server(models, slots=4)
+    mixed = srv.serve(reqs)
+    assert not srv.errors, srv.errors
     assert len(mixed) == len(reqs)
     alone = []
     for r in reqs:  # one at a time, nothing else on the device
