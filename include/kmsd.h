@@ -113,6 +113,13 @@ int kmsd_csr_create(int64_t n, const int64_t *indptr, const int64_t *indices,
 void kmsd_csr_destroy(kmsd_csr a);
 int64_t kmsd_csr_rows(kmsd_csr a);
 int64_t kmsd_csr_nnz(kmsd_csr a);
+/* Device storage forms built at upload besides CSR, as a bit mask:
+ * KMSD_FORM_ELL (padded rows of width <= 32, padding <= 25%) and
+ * KMSD_FORM_BSR4 (dense 4x4 blocks, zero fill <= 25%).  No counterpart in the
+ * reference, which keeps CSR only; -1 for a null handle. */
+#define KMSD_FORM_ELL 1
+#define KMSD_FORM_BSR4 2
+int kmsd_csr_forms(kmsd_csr a);
 
 /* Y = A X for device complex128 X, Y of shape (n, b).  Replaces CSR::mul /
  * `CSR.matmul` (cpp/native.cpp:75-89, 642-646).  X and Y must not overlap. */

@@ -19,6 +19,7 @@ HEADER = Path(__file__).resolve().parent.parent / "include" / "kmsd.h"
 KMSD_OK, KMSD_EINVAL, KMSD_ERUNTIME, KMSD_EMETRIC, KMSD_ECUDA = 0, 1, 2, 3, 4
 KMSD_FP64, KMSD_MIXED = 0, 1
 KMSD_MOMENTS_DIRECT, KMSD_MOMENTS_DOUBLING = 0, 1
+KMSD_FORM_ELL, KMSD_FORM_BSR4 = 1, 2
 
 
 class SolveReport(C.Structure):
@@ -49,6 +50,7 @@ SIGNATURES = {
     "kmsd_csr_destroy": (None, [P]),
     "kmsd_csr_rows": (I64, [P]),
     "kmsd_csr_nnz": (I64, [P]),
+    "kmsd_csr_forms": (C.c_int, [P]),
     "kmsd_csr_matmul": (C.c_int, [P, P, P, I64, P]),
     "kmsd_metric_create": (C.c_int, [P, PD, I64, PI64, PI64, PD, PD, C.POINTER(P)]),
     "kmsd_metric_destroy": (None, [P]),

@@ -319,8 +319,6 @@ int run_batch(kmsd_batch_s *bt, const double2 *B, double *mu, int64_t b, int64_t
         switch (mu_n) {
             case 1: return record<T, 1>(bt, B, mu, b, length, doubling, s, k);
             case 2: return record<T, 2>(bt, B, mu, b, length, doubling, s, k);
-            case 4: return record<T, 4>(bt, B, mu, b, length, doubling, s, k);
-            case 8: return record<T, 8>(bt, B, mu, b, length, doubling, s, k);
         }
         return fail(KMSD_EINVAL, "too many columns for one batch call");
     };

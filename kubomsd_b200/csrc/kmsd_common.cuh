@@ -5,7 +5,7 @@
 // 16-byte "units": one complex128 (double2) or two complex64 (float4), so
 // every global access is a 128-bit load or store.  A row of b columns is
 // U = b / C units; a "row group" of G threads (G = next power of two >= U,
-// at most 32) walks rows with a grid stride, each lane owning the units
+// at most 128) walks rows with a grid stride, each lane owning the units
 // lane, lane + G, ... of the row.
 #pragma once
 
@@ -89,9 +89,20 @@ template <class T> struct EllView {
     int w;        // 0: no ELL form
 };
 
+// The same matrix as block CSR with dense 4x4 blocks (the atom blocks of an
+// sp3 basis): block row I covers rows 4I..4I+3; each block's 16 values are
+// stored row-major, absent entries as zeros.  nbrows == 0 when not built.
+template <class T> struct BsrView {
+    const int *bptr;  // nbrows + 1
+    const int *bidx;  // block column of each block
+    const T *re;      // 16 values per block
+    const T *im;      // nullptr for a real matrix
+    int64_t nbrows;
+};
+
 // ---------------------------------------------------------------- mapping
 struct RowMap {
-    int G;      // threads per row group (power of two, <= 32)
+    int G;      // threads per row group (power of two, <= 128)
     int gpc;    // row groups per CTA
     int U;      // units per row
 };
@@ -234,11 +245,25 @@ __device__ __forceinline__ void final_column_sums(const double2 *partial, int np
         if (part < split) {
             const int per = (nparts + split - 1) / split;
             const int lo = part * per, hi = min(nparts, lo + per);
-            for (int p = lo; p < hi; ++p) {
-                const double2 v = __ldcg(partial + (size_t)p * ncol + c0 + col);
-                sx += v.x;
-                sy += v.y;
+            // four independent chains keep four loads in flight; they are
+            // combined in a fixed order, so the sum does not depend on timing
+            double ax[4] = {0., 0., 0., 0.}, ay[4] = {0., 0., 0., 0.};
+            int p = lo;
+            for (; p + 4 <= hi; p += 4) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const double2 v = __ldcg(partial + (size_t)(p + q) * ncol + c0 + col);
+                    ax[q] += v.x;
+                    ay[q] += v.y;
+                }
             }
+            for (; p < hi; ++p) {
+                const double2 v = __ldcg(partial + (size_t)p * ncol + c0 + col);
+                ax[0] += v.x;
+                ay[0] += v.y;
+            }
+            sx = (ax[0] + ax[1]) + (ax[2] + ax[3]);
+            sy = (ay[0] + ay[1]) + (ay[2] + ay[3]);
         }
         __syncthreads();
         if (part < split) smem[part * cols + col] = make_double2(sx, sy);
@@ -260,9 +285,75 @@ __device__ __forceinline__ void final_column_max(const double *partial, int npar
                                                  double *out) {
     for (int col = threadIdx.x; col < ncol; col += blockDim.x) {
         double s = 0.;
+#pragma unroll 8
         for (int p = 0; p < nparts; ++p) s = fmax(s, __ldcg(partial + (size_t)p * ncol + col));
         out[col] = s;
     }
+}
+
+// ------------------------------------------------------- two-level combination
+// In a short kernel (one PCG iteration on a few 10^4 rows takes
+// microseconds) a last CTA that reads all ~10^3 partial rows is the critical
+// path.  Instead the CTAs form groups of kTreeFan consecutive CTAs: the last
+// CTA of a group to arrive combines the group's rows in a fixed order into a
+// level-2 row partial[(gridDim.x + group) * ncol + col], and the last group
+// to arrive combines the level-2 rows in a fixed order into out.  The result
+// is the same in every run, and each step reads at most kTreeFan rows per
+// column.  Tickets: tk[0] for the root, tk[1 + group] per group; all are
+// left at zero.  The partial array needs tree_rows(gridDim.x) rows.
+constexpr int kTreeFan = 32;
+constexpr int kTreeTickets = 1024;  // tickets in a reduction's ticket array
+__host__ __device__ inline int tree_rows(int grid) { return grid + (grid + kTreeFan - 1) / kTreeFan; }
+
+// True in the CTA that is the `expected`-th to arrive at ticket t; its reads
+// after the return see every arrived CTA's writes.  Resets the ticket.
+__device__ __forceinline__ bool arrive_last(Ticket *t, unsigned expected) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = atomicAdd(&t->count, 1u) == expected - 1;
+    __syncthreads();
+    if (is_last) {
+        __threadfence();
+        if (threadIdx.x == 0) t->count = 0;
+    }
+    return is_last;
+}
+
+__device__ __forceinline__ bool tree_column_sums(double2 *partial, int ncol, Ticket *tk, double2 *smem,
+                                                 double2 *out) {
+    const int grid = gridDim.x;
+    const int ngroups = (grid + kTreeFan - 1) / kTreeFan;
+    if (ngroups == 1) {
+        if (!arrive_last(tk, grid)) return false;
+        final_column_sums(partial, grid, ncol, smem, out);
+        return true;
+    }
+    const int group = blockIdx.x / kTreeFan, lo = group * kTreeFan, cnt = min(kTreeFan, grid - lo);
+    if (!arrive_last(tk + 1 + group, cnt)) return false;
+    double2 *level2 = partial + (size_t)grid * ncol;
+    final_column_sums(partial + (size_t)lo * ncol, cnt, ncol, smem, level2 + (size_t)group * ncol);
+    if (!arrive_last(tk, ngroups)) return false;
+    final_column_sums(level2, ngroups, ncol, smem, out);
+    return true;
+}
+
+__device__ __forceinline__ bool tree_column_max(double *partial, int ncol, Ticket *tk, double *out) {
+    const int grid = gridDim.x;
+    const int ngroups = (grid + kTreeFan - 1) / kTreeFan;
+    if (ngroups == 1) {
+        if (!arrive_last(tk, grid)) return false;
+        final_column_max(partial, grid, ncol, out);
+        return true;
+    }
+    const int group = blockIdx.x / kTreeFan, lo = group * kTreeFan, cnt = min(kTreeFan, grid - lo);
+    if (!arrive_last(tk + 1 + group, cnt)) return false;
+    double *level2 = partial + (size_t)grid * ncol;
+    final_column_max(partial + (size_t)lo * ncol, cnt, ncol, level2 + (size_t)group * ncol);
+    __syncthreads();
+    if (!arrive_last(tk, ngroups)) return false;
+    final_column_max(level2, ngroups, ncol, out);
+    return true;
 }
 
 // ---------------------------------------------------------------- host errors

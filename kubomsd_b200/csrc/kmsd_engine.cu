@@ -98,13 +98,12 @@ int wave_grid(const void *kernel, size_t smem, int64_t rows, const RowMap &mp) {
 }
 int mu_for(const RowMap &mp) {
     // At most 256 units (512 reduction columns) per launch: the fixed-size
-    // shared buffers of the reductions are sized for that.
+    // shared buffers of the reductions are sized for that.  Row groups are up
+    // to 128 lanes wide, so a lane holds one or two units.
     if (mp.U > 256) return 0;
     const int per = (mp.U + mp.G - 1) / mp.G;
     if (per <= 1) return 1;
     if (per <= 2) return 2;
-    if (per <= 4) return 4;
-    if (per <= 8) return 8;
     return 0;
 }
 size_t reduce_smem(const RowMap &mp, int C) {
@@ -112,10 +111,10 @@ size_t reduce_smem(const RowMap &mp, int C) {
     return std::max(a, b) * sizeof(double2);
 }
 int Reducer::ensure(int grid, int ncol, int copies) {
-    if (partial.ensure((size_t)grid * ncol * copies * sizeof(double2) + 64)) return KMSD_ECUDA;
+    if (partial.ensure((size_t)tree_rows(grid) * ncol * copies * sizeof(double2) + 64)) return KMSD_ECUDA;
     if (!ticket.p) {
-        if (ticket.ensure(64)) return KMSD_ECUDA;
-        KMSD_CUDA(cudaMemset(ticket.p, 0, 64));
+        if (ticket.ensure(kTreeTickets * sizeof(Ticket))) return KMSD_ECUDA;
+        KMSD_CUDA(cudaMemset(ticket.p, 0, kTreeTickets * sizeof(Ticket)));
     }
     return KMSD_OK;
 }
@@ -179,8 +178,6 @@ int spmm_any(CsrView<T> A, const typename Unit<T>::vec *X, typename Unit<T>::vec
     switch (mu) {
         KMSD_SPMM_CASE(1)
         KMSD_SPMM_CASE(2)
-        KMSD_SPMM_CASE(4)
-        KMSD_SPMM_CASE(8)
     }
 #undef KMSD_SPMM_CASE
     KMSD_CUDA(cudaGetLastError());
@@ -190,6 +187,38 @@ int spmm_any(CsrView<T> A, const typename Unit<T>::vec *X, typename Unit<T>::vec
 
 namespace kmsd {
 int spmm64(const kmsd_csr_s *A, const double2 *X, double2 *Y, int64_t b, cudaStream_t s, double2 *dot_out) {
+    if (A->bsr_nb > 0) {
+        static thread_local Reducer red;
+        const RowMap mp = make_map((int)b, kThreads);
+        const int mu = mu_for(mp);
+        if (!mu) return fail(KMSD_EINVAL, "too many columns for one SpMM call");
+        const int grid = grid_for(A->bsr_nb, mp);
+        if (red.ensure(grid, (int)b)) return KMSD_ECUDA;
+        const size_t sm = reduce_smem(mp, 1);
+        const BsrView<double> v = A->bsr64();
+        const bool cplx = v.im != nullptr;
+#define KMSD_BSR_LAUNCH(M, D, Z) \
+    spmm_bsr_kernel<M, D, Z><<<grid, kThreads, sm, s>>>(v, X, Y, mp, red.part(), red.tick(), D ? dot_out : nullptr)
+#define KMSD_BSR_CASE(M)                              \
+    case M:                                           \
+        if (dot_out) {                                \
+            if (cplx) KMSD_BSR_LAUNCH(M, true, true); \
+            else KMSD_BSR_LAUNCH(M, true, false);     \
+        } else {                                      \
+            if (cplx) KMSD_BSR_LAUNCH(M, false, true); \
+            else KMSD_BSR_LAUNCH(M, false, false);    \
+        }                                             \
+        break;
+        switch (mu) {
+            KMSD_BSR_CASE(1)
+            KMSD_BSR_CASE(2)
+        }
+#undef KMSD_BSR_CASE
+#undef KMSD_BSR_LAUNCH
+        count_launch();
+        KMSD_CUDA(cudaGetLastError());
+        return KMSD_OK;
+    }
     return spmm_any<double>(A->view64(), X, Y, A->n, (int)b, s, dot_out);
 }
 int spmm32(const kmsd_csr_s *A, const float4 *X, float4 *Y, int64_t U, cudaStream_t s, double2 *dot_out) {
@@ -245,7 +274,7 @@ __global__ void __launch_bounds__(256) coldot_kernel(const typename Unit<T>::vec
     }
     const int ncol = mp.U * C;
     cta_column_sums<MU, C>(acc, mp, ncol, smem, partial);
-    if (last_cta(tk)) final_column_sums(partial, gridDim.x, ncol, smem, out);
+    tree_column_sums(partial, ncol, tk, smem, out);
 }
 
 template <class T>
@@ -261,8 +290,6 @@ int coldot_any(const typename Unit<T>::vec *x, const typename Unit<T>::vec *y, i
     switch (mu) {
         case 1: coldot_kernel<T, 1><<<grid, kThreads, sm, s>>>(x, y, n, mp, red.part(), red.tick(), out); break;
         case 2: coldot_kernel<T, 2><<<grid, kThreads, sm, s>>>(x, y, n, mp, red.part(), red.tick(), out); break;
-        case 4: coldot_kernel<T, 4><<<grid, kThreads, sm, s>>>(x, y, n, mp, red.part(), red.tick(), out); break;
-        case 8: coldot_kernel<T, 8><<<grid, kThreads, sm, s>>>(x, y, n, mp, red.part(), red.tick(), out); break;
     }
     count_launch();
     KMSD_CUDA(cudaGetLastError());
@@ -368,6 +395,51 @@ int kmsd_csr_create(int64_t n, const int64_t *indptr, const int64_t *indices, co
         if (!rc && cplx) rc = up((void **)&A->ell_im64, eim.data(), m * sizeof(double));
         if (!rc) A->ell_w = (int)w;
     }
+    // 4x4 block-CSR form when the pattern tiles into aligned 4x4 blocks (the
+    // atom blocks of an sp3 basis) with at most a quarter of zero fill over
+    // the matrix, and no block row more than doubled: each gathered input row
+    // then serves four output rows.
+    if (!rc && !ident && n % 4 == 0 && nnz >= 16) {
+        const int64_t nbr = n / 4;
+        std::vector<int> bptr(nbr + 1, 0), bcols;
+        std::vector<int64_t> mark(nbr, -1);
+        bool ok = true;
+        for (int64_t I = 0; I < nbr && ok; ++I) {
+            const size_t start = bcols.size();
+            for (int64_t r = 4 * I; r < 4 * I + 4; ++r)
+                for (int64_t k = indptr[r]; k < indptr[r + 1]; ++k) {
+                    const int64_t J = indices[k] / 4;
+                    if (mark[J] != I) {
+                        mark[J] = I;
+                        bcols.push_back((int)J);
+                    }
+                }
+            std::sort(bcols.begin() + start, bcols.end());
+            const int64_t row_nnz = indptr[4 * I + 4] - indptr[4 * I];
+            ok = (int64_t)(bcols.size() - start) * 16 <= 2 * row_nnz + 16 && bcols.size() < (size_t)INT32_MAX / 16;
+            bptr[I + 1] = (int)bcols.size();
+        }
+        const int64_t nblk = (int64_t)bcols.size();
+        if (ok && nblk * 16 <= nnz + nnz / 4) {
+            std::vector<double> br((size_t)nblk * 16, 0.), bi(cplx ? (size_t)nblk * 16 : 0, 0.);
+            for (int64_t I = 0; I < nbr; ++I) {
+                const int *b0 = bcols.data() + bptr[I], *b1 = bcols.data() + bptr[I + 1];
+                for (int64_t r = 4 * I; r < 4 * I + 4; ++r)
+                    for (int64_t k = indptr[r]; k < indptr[r + 1]; ++k) {
+                        const int J = (int)(indices[k] / 4);
+                        const int64_t q = std::lower_bound(b0, b1, J) - bcols.data();
+                        const size_t e = (size_t)q * 16 + (size_t)(r - 4 * I) * 4 + (size_t)(indices[k] - 4 * J);
+                        br[e] += val_re[k];
+                        if (cplx) bi[e] += val_im[k];
+                    }
+            }
+            rc = up((void **)&A->bsr_ptr, bptr.data(), (nbr + 1) * sizeof(int));
+            if (!rc) rc = up((void **)&A->bsr_idx, bcols.data(), nblk * sizeof(int));
+            if (!rc) rc = up((void **)&A->bsr_re, br.data(), br.size() * sizeof(double));
+            if (!rc && cplx) rc = up((void **)&A->bsr_im, bi.data(), bi.size() * sizeof(double));
+            if (!rc) A->bsr_nb = nbr;
+        }
+    }
     if (rc) {
         kmsd_csr_destroy(A);
         return rc;
@@ -389,11 +461,19 @@ void kmsd_csr_destroy(kmsd_csr a) {
     cudaFree(a->ell_im64);
     cudaFree(a->ell_re32);
     cudaFree(a->ell_im32);
+    cudaFree(a->bsr_ptr);
+    cudaFree(a->bsr_idx);
+    cudaFree(a->bsr_re);
+    cudaFree(a->bsr_im);
     delete a;
 }
 
 int64_t kmsd_csr_rows(kmsd_csr a) { return a ? a->n : -1; }
 int64_t kmsd_csr_nnz(kmsd_csr a) { return a ? a->nnz : -1; }
+int kmsd_csr_forms(kmsd_csr a) {
+    if (!a) return -1;
+    return (a->ell_w > 0 ? KMSD_FORM_ELL : 0) | (a->bsr_nb > 0 ? KMSD_FORM_BSR4 : 0);
+}
 
 int kmsd_csr_matmul(kmsd_csr a, const void *x, void *y, int64_t b, void *stream) {
     if (!a || !x || !y || b < 1) return fail(KMSD_EINVAL, "CSR input dimension mismatch");

@@ -41,7 +41,8 @@ int grid_for(int64_t rows, const RowMap &mp);
 // Grid of one resident wave of `kernel` (occupancy API; cached per kernel and
 // shared-memory size), capped by the row groups needed.
 int wave_grid(const void *kernel, size_t smem, int64_t rows, const RowMap &mp);
-// Units per thread bucket {1,2,4,8}; 0 when too wide.
+// Units per lane: 1 or 2 (row groups are up to 128 lanes, rows up to 256
+// units); 0 when too wide.
 int mu_for(const RowMap &mp);
 size_t reduce_smem(const RowMap &mp, int C);
 
@@ -61,11 +62,18 @@ struct kmsd_csr_s {
     int *ell_idx = nullptr;
     double *ell_re64 = nullptr, *ell_im64 = nullptr;
     float *ell_re32 = nullptr, *ell_im32 = nullptr;
+    // 4x4 block-CSR copy (see BsrView); bsr_nb == 0 when not built.
+    int64_t bsr_nb = 0;
+    int *bsr_ptr = nullptr, *bsr_idx = nullptr;
+    double *bsr_re = nullptr, *bsr_im = nullptr;
     int ensure_f32();
     kmsd::CsrView<double> view64() const { return {ptr, idx, re64, complex_values ? im64 : nullptr}; }
     kmsd::CsrView<float> view32() const { return {ptr, idx, re32, complex_values ? im32 : nullptr}; }
     kmsd::EllView<double> ell64() const { return {ell_idx, ell_re64, complex_values ? ell_im64 : nullptr, ell_w}; }
     kmsd::EllView<float> ell32() const { return {ell_idx, ell_re32, complex_values ? ell_im32 : nullptr, ell_w}; }
+    kmsd::BsrView<double> bsr64() const {
+        return {bsr_ptr, bsr_idx, bsr_re, complex_values ? bsr_im : nullptr, bsr_nb};
+    }
 };
 
 namespace kmsd {

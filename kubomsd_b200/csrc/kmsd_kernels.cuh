@@ -104,6 +104,86 @@ __device__ __forceinline__ void gather_row_ell(const EllView<T> &A, const typena
     }
 }
 
+// acc[i][m] += sum over the 4x4 blocks of block row I of A[4I+i, 4J+j] X[4J+j, u_m]:
+// each gathered input row serves four output rows from registers.  CPLX
+// selects complex block values at compile time, so a real matrix (the usual
+// tight-binding S and H) carries no registers for imaginary parts; block
+// values are loaded one block row at a time.
+template <int MU, bool CPLX>
+__device__ __forceinline__ void gather_block_row(const BsrView<double> &A, const double2 *X, int64_t I, int U,
+                                                 int G, int lane, Pk<double> (&acc)[4][MU]) {
+    const int k0 = __ldg(A.bptr + I), k1 = __ldg(A.bptr + I + 1);
+    for (int k = k0; k < k1; ++k) {
+        const int J = __ldg(A.bidx + k);
+        Pk<double> x[MU][4];
+#pragma unroll
+        for (int m = 0; m < MU; ++m) {
+            const int u = lane + m * G;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) x[m][j] = u < U ? ldg(X + (size_t)(4 * J + j) * U + u) : pk_zero<double>();
+        }
+        const double2 *pr = reinterpret_cast<const double2 *>(A.re + (size_t)k * 16);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const double2 r01 = __ldg(pr + 2 * i), r23 = __ldg(pr + 2 * i + 1);
+            const double vr[4] = {r01.x, r01.y, r23.x, r23.y};
+            if constexpr (CPLX) {
+                const double2 *pi = reinterpret_cast<const double2 *>(A.im + (size_t)k * 16);
+                const double2 i01 = __ldg(pi + 2 * i), i23 = __ldg(pi + 2 * i + 1);
+                const double vi[4] = {i01.x, i01.y, i23.x, i23.y};
+#pragma unroll
+                for (int m = 0; m < MU; ++m)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) cmac_cplx(acc[i][m], vr[j], vi[j], x[m][j]);
+            } else {
+#pragma unroll
+                for (int m = 0; m < MU; ++m)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) cmac_real(acc[i][m], vr[j], x[m][j]);
+            }
+        }
+    }
+}
+
+// Y = A X over the block rows of a 4x4 BSR matrix (optionally with the
+// conj(X_row) * Y_row column sums, as spmm_kernel).
+template <int MU, bool DOT, bool CPLX>
+__global__ void __launch_bounds__(256) spmm_bsr_kernel(BsrView<double> A, const double2 *X, double2 *Y, RowMap mp,
+                                                       double2 *partial, Ticket *ticket, double2 *dot_out) {
+    extern __shared__ double2 smem[];
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    double2 acc[MU][1];
+#pragma unroll
+    for (int m = 0; m < MU; ++m) acc[m][0] = make_double2(0., 0.);
+    for (int64_t I = (int64_t)blockIdx.x * mp.gpc + g; I < A.nbrows; I += (int64_t)gridDim.x * mp.gpc) {
+        Pk<double> y[4][MU];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int m = 0; m < MU; ++m) y[i][m] = pk_zero<double>();
+        gather_block_row<MU, CPLX>(A, X, I, mp.U, mp.G, lane, y);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int m = 0; m < MU; ++m) {
+                const int u = lane + m * mp.G;
+                if (u < mp.U) {
+                    const size_t o = (size_t)(4 * I + i) * mp.U + u;
+                    st(Y + o, y[i][m]);
+                    if (DOT) {
+                        const Pk<double> x = ld(X + o);
+                        acc[m][0].x += x.re[0] * y[i][m].re[0] + x.im[0] * y[i][m].im[0];
+                        acc[m][0].y += x.re[0] * y[i][m].im[0] - x.im[0] * y[i][m].re[0];
+                    }
+                }
+            }
+    }
+    if (DOT) {
+        cta_column_sums<MU, 1>(acc, mp, mp.U, smem, partial);
+        tree_column_sums(partial, mp.U, ticket, smem, dot_out);
+    }
+}
+
 // Same for one unit (runtime loop callers).
 template <class T>
 __device__ __forceinline__ Pk<T> gather_unit(const CsrView<T> &A, const typename Unit<T>::vec *X,
@@ -162,7 +242,7 @@ __global__ void __launch_bounds__(256) spmm_kernel(CsrView<T> A, const typename 
     if (DOT) {
         const int ncol = mp.U * C;
         cta_column_sums<MU, C>(acc, mp, ncol, smem, partial);
-        if (last_cta(ticket)) final_column_sums(partial, gridDim.x, ncol, smem, dot_out);
+        tree_column_sums(partial, ncol, ticket, smem, dot_out);
     }
 }
 

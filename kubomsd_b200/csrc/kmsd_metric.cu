@@ -179,8 +179,7 @@ __global__ void __launch_bounds__(256) pcg_scale_kernel(const double2 *B, int64_
     }
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(c.flags + 2, 1);
     cta_column_max<MU, 1>(acc, mp, mp.U, smem, partial);
-    if (last_cta(tk)) {
-        final_column_max(partial, gridDim.x, mp.U, c.safe);
+    if (tree_column_max(partial, mp.U, tk, c.safe)) {
         __syncthreads();
         for (int j = threadIdx.x; j < mp.U; j += blockDim.x)
             if (c.safe[j] == 0.) c.safe[j] = 1.;
@@ -231,9 +230,8 @@ __global__ void __launch_bounds__(256) pcg_init_kernel(const double2 *B, double2
         }
     }
     cta_column_sums<MU, 1>(acc, mp, U, smem, partial);
-    if (last_cta(tk)) {
-        __shared__ double2 tot[256];
-        final_column_sums(partial, gridDim.x, U, smem, tot);
+    __shared__ double2 tot[256];
+    if (tree_column_sums(partial, U, tk, smem, tot)) {
         __syncthreads();
         const int j = threadIdx.x;
         bool act = false;
@@ -270,9 +268,41 @@ __global__ void pcg_pinit_kernel(const double2 *z, double2 *p, int64_t len, int 
     }
 }
 
+// Storage form of S in the S products: CSR, or 4x4 blocks with real or
+// complex values.
+enum { S_CSR = 0, S_BSR_REAL = 1, S_BSR_CPLX = 2 };
+
+// Calls f(row, yv) for every row owned by this thread's row group, with
+// yv[m] = (S X)[row, unit lane + m*G], from CSR or from 4x4 blocks (a block
+// row's four rows share every gathered input row).
+template <int MU, int SF, class F>
+__device__ __forceinline__ void for_rows_spmv(const CsrView<double> &S, const BsrView<double> &SB, const double2 *X,
+                                              int64_t n, const RowMap &mp, int g, int lane, F &&f) {
+    if constexpr (SF != S_CSR) {
+        for (int64_t I = (int64_t)blockIdx.x * mp.gpc + g; I < SB.nbrows; I += (int64_t)gridDim.x * mp.gpc) {
+            Pk<double> acc4[4][MU];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int m = 0; m < MU; ++m) acc4[i][m] = pk_zero<double>();
+            gather_block_row<MU, SF == S_BSR_CPLX>(SB, X, I, mp.U, mp.G, lane, acc4);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) f(4 * I + i, acc4[i]);
+        }
+    } else {
+        for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < n; row += (int64_t)gridDim.x * mp.gpc) {
+            Pk<double> yv[MU];
+#pragma unroll
+            for (int m = 0; m < MU; ++m) yv[m] = pk_zero<double>();
+            gather_row<double, MU>(S, X, row, mp.U, mp.G, lane, yv);
+            f(row, yv);
+        }
+    }
+}
+
 // ---- sp = S p, curvature <p, sp>, alpha, breakdown
-template <int MU>
-__global__ void __launch_bounds__(256) pcg_spmv_kernel(CsrView<double> S, const double2 *p, double2 *sp,
+template <int MU, int SF>
+__global__ void __launch_bounds__(256) pcg_spmv_kernel(CsrView<double> S, BsrView<double> SB, const double2 *p, double2 *sp,
                                                        int64_t n, RowMap mp, ColPtr c, double2 *partial,
                                                        Ticket *tk) {
     if (*(volatile int *)c.flags) return;
@@ -280,11 +310,7 @@ __global__ void __launch_bounds__(256) pcg_spmv_kernel(CsrView<double> S, const 
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
     double2 acc[MU][1];
     ZERO_ACC(acc);
-    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < n; row += (int64_t)gridDim.x * mp.gpc) {
-        Pk<double> yv[MU];
-#pragma unroll
-        for (int m = 0; m < MU; ++m) yv[m] = pk_zero<double>();
-        gather_row<double, MU>(S, p, row, mp.U, mp.G, lane, yv);
+    for_rows_spmv<MU, SF>(S, SB, p, n, mp, g, lane, [&](int64_t row, const Pk<double>(&yv)[MU]) {
 #pragma unroll
         for (int m = 0; m < MU; ++m) {
             const int u = lane + m * mp.G;
@@ -296,11 +322,10 @@ __global__ void __launch_bounds__(256) pcg_spmv_kernel(CsrView<double> S, const 
                 acc[m][0].y += x.x * yv[m].im[0] - x.y * yv[m].re[0];
             }
         }
-    }
+    });
     cta_column_sums<MU, 1>(acc, mp, mp.U, smem, partial);
-    if (last_cta(tk)) {
-        __shared__ double2 tot[256];
-        final_column_sums(partial, gridDim.x, mp.U, smem, tot);
+    __shared__ double2 tot[256];
+    if (tree_column_sums(partial, mp.U, tk, smem, tot)) {
         __syncthreads();
         const int j = threadIdx.x;
         bool b = false;
@@ -368,9 +393,8 @@ __global__ void __launch_bounds__(256) pcg_update_kernel(double2 *y, double2 *r,
         }
     }
     cta_column_sums<MU, 1>(acc, mp, U, smem, partial);
-    if (last_cta(tk)) {
-        __shared__ double2 tot[256];
-        final_column_sums(partial, gridDim.x, U, smem, tot);
+    __shared__ double2 tot[256];
+    if (tree_column_sums(partial, U, tk, smem, tot)) {
         __syncthreads();
         const int j = threadIdx.x;
         bool cand = false;
@@ -409,8 +433,9 @@ __global__ void __launch_bounds__(256) pcg_update_kernel(double2 *y, double2 *r,
 }
 
 // ---- true residual t = q - S y; sums |t|^2 and |t - r|^2; refresh decision
-template <int MU>
-__global__ void __launch_bounds__(256) pcg_true_residual_kernel(CsrView<double> S, const double2 *q,
+template <int MU, int SF>
+__global__ void __launch_bounds__(256) pcg_true_residual_kernel(CsrView<double> S, BsrView<double> SB,
+                                                                const double2 *q,
                                                                 const double2 *y, const double2 *r, double2 *t,
                                                                 int64_t n, RowMap mp, ColPtr c, int adaptive,
                                                                 double gap_ratio, double2 *partial, Ticket *tk,
@@ -420,11 +445,7 @@ __global__ void __launch_bounds__(256) pcg_true_residual_kernel(CsrView<double> 
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
     double2 acc[MU][1];
     ZERO_ACC(acc);
-    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < n; row += (int64_t)gridDim.x * mp.gpc) {
-        Pk<double> sy[MU];
-#pragma unroll
-        for (int m = 0; m < MU; ++m) sy[m] = pk_zero<double>();
-        gather_row<double, MU>(S, y, row, mp.U, mp.G, lane, sy);
+    for_rows_spmv<MU, SF>(S, SB, y, n, mp, g, lane, [&](int64_t row, const Pk<double>(&sy)[MU]) {
 #pragma unroll
         for (int m = 0; m < MU; ++m) {
             const int u = lane + m * mp.G;
@@ -438,11 +459,10 @@ __global__ void __launch_bounds__(256) pcg_true_residual_kernel(CsrView<double> 
                 acc[m][0].y += dx * dx + dy * dy;
             }
         }
-    }
+    });
     cta_column_sums<MU, 1>(acc, mp, mp.U, smem, partial);
-    if (last_cta(tk)) {
-        __shared__ double2 tot[256];
-        final_column_sums(partial, gridDim.x, mp.U, smem, tot);
+    __shared__ double2 tot[256];
+    if (tree_column_sums(partial, mp.U, tk, smem, tot)) {
         __syncthreads();
         const int j = threadIdx.x;
         bool rs = false;
@@ -517,9 +537,8 @@ __global__ void __launch_bounds__(256) pcg_restart_kernel(double2 *r, double2 *z
         }
     }
     cta_column_sums<MU, 1>(acc, mp, U, smem, partial);
-    if (last_cta(tk)) {
-        __shared__ double2 tot[256];
-        final_column_sums(partial, gridDim.x, U, smem, tot);
+    __shared__ double2 tot[256];
+    if (tree_column_sums(partial, U, tk, smem, tot)) {
         __syncthreads();
         const int j = threadIdx.x;
         bool act = false;
@@ -560,19 +579,15 @@ __global__ void pcg_direction_kernel(const double2 *z, double2 *p, int64_t len, 
 }
 
 // ---- final acceptance: t = q - S y; converged, relative, residual
-template <int MU>
-__global__ void __launch_bounds__(256) pcg_final_kernel(CsrView<double> S, const double2 *q, const double2 *y,
+template <int MU, int SF>
+__global__ void __launch_bounds__(256) pcg_final_kernel(CsrView<double> S, BsrView<double> SB, const double2 *q, const double2 *y,
                                                         int64_t n, RowMap mp, ColPtr c, double2 *partial,
                                                         Ticket *tk, Counters *cnt) {
     extern __shared__ double2 smem[];
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
     double2 acc[MU][1];
     ZERO_ACC(acc);
-    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < n; row += (int64_t)gridDim.x * mp.gpc) {
-        Pk<double> sy[MU];
-#pragma unroll
-        for (int m = 0; m < MU; ++m) sy[m] = pk_zero<double>();
-        gather_row<double, MU>(S, y, row, mp.U, mp.G, lane, sy);
+    for_rows_spmv<MU, SF>(S, SB, y, n, mp, g, lane, [&](int64_t row, const Pk<double>(&sy)[MU]) {
 #pragma unroll
         for (int m = 0; m < MU; ++m) {
             const int u = lane + m * mp.G;
@@ -582,11 +597,10 @@ __global__ void __launch_bounds__(256) pcg_final_kernel(CsrView<double> S, const
                 acc[m][0].x += tx * tx + ty * ty;
             }
         }
-    }
+    });
     cta_column_sums<MU, 1>(acc, mp, mp.U, smem, partial);
-    if (last_cta(tk)) {
-        __shared__ double2 tot[256];
-        final_column_sums(partial, gridDim.x, mp.U, smem, tot);
+    __shared__ double2 tot[256];
+    if (tree_column_sums(partial, mp.U, tk, smem, tot)) {
         __syncthreads();
         const int j = threadIdx.x;
         if (j < mp.U) {
@@ -625,9 +639,8 @@ __global__ void __launch_bounds__(256) pcg_out_kernel(const double2 *y, double2 
         }
     }
     cta_column_sums<MU, 1>(acc, mp, mp.U, smem, partial);
-    if (last_cta(tk)) {
-        __shared__ double2 tot[256];
-        final_column_sums(partial, gridDim.x, mp.U, smem, tot);
+    __shared__ double2 tot[256];
+    if (tree_column_sums(partial, mp.U, tk, smem, tot)) {
         __syncthreads();
         const int j = threadIdx.x;
         bool notconv = false, unrep = false;
@@ -719,13 +732,16 @@ int kmsd_metric_s::ensure(int64_t b) {
 
 namespace {
 
-template <int MU, int MAXB>
+template <int MU, int MAXB, int SF>
 int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rtol, double atol, int maxiter,
             cudaStream_t s, int *status, FailReportFull *fr, int *claimed) {
     const int64_t n = M->n;
     const RowMap mp = make_map((int)b, kThreads);
     const int64_t nb = MAXB == 1 ? n : M->nblocks;
     const int grid_r = grid_for(n, mp), grid_b = grid_for(nb, mp);
+    // S products walk block rows when S is stored as 4x4 blocks
+    const int grid_s = SF != S_CSR ? grid_for(M->S->bsr_nb, mp) : grid_r;
+    const BsrView<double> SB = M->S->bsr64();
     const int grid_mx = grid_r > grid_b ? grid_r : grid_b;
     if (M->red.ensure(grid_mx, (int)b)) return KMSD_ECUDA;
     const size_t sm = reduce_smem(mp, 1);
@@ -752,14 +768,14 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
     int slot = 0, pending = 0;
     for (int k = 0; k < maxiter; ++k) {
         const int refresh = ((k + 1) % M->interval) == 0;
-        pcg_spmv_kernel<MU><<<grid_r, kThreads, sm, s>>>(S, p, sp, n, mp, c, part, tk);
+        pcg_spmv_kernel<MU, SF><<<grid_s, kThreads, sm, s>>>(S, SB, p, sp, n, mp, c, part, tk);
         count_launch();
         pcg_update_kernel<MU, MAXB><<<grid_b, kThreads, sm, s>>>(y, r, z, p, sp, P, nb, mp, c, refresh,
                                                                  M->adaptive, part, tk);
         count_launch();
         if (refresh || M->adaptive) {
-            pcg_true_residual_kernel<MU><<<grid_r, kThreads, sm, s>>>(S, q, y, r, t, n, mp, c, M->adaptive,
-                                                                     M->gap_ratio, part, tk, cnt);
+            pcg_true_residual_kernel<MU, SF><<<grid_s, kThreads, sm, s>>>(S, SB, q, y, r, t, n, mp, c,
+                                                                         M->adaptive, M->gap_ratio, part, tk, cnt);
             count_launch();
             pcg_restart_kernel<MU, MAXB><<<grid_b, kThreads, sm, s>>>(r, z, t, P, nb, mp, c, part, tk);
             count_launch();
@@ -779,7 +795,7 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
         }
     }
     KMSD_CUDA(cudaGetLastError());
-    pcg_final_kernel<MU><<<grid_r, kThreads, sm, s>>>(S, q, y, n, mp, c, part, tk, cnt);
+    pcg_final_kernel<MU, SF><<<grid_s, kThreads, sm, s>>>(S, SB, q, y, n, mp, c, part, tk, cnt);
     count_launch();
     pcg_out_kernel<MU><<<grid_r, kThreads, sm, s>>>(y, Y, n, mp, c, part, tk, cnt, status, fr);
     count_launch();
@@ -794,22 +810,28 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
 using PcgFn = int (*)(kmsd_metric_s *, const double2 *, double2 *, int64_t, double, double, int, cudaStream_t,
                       int *, FailReportFull *, int *);
 
-template <int MAXB>
+template <int MAXB, int SF>
 PcgFn pick_mu(int mu) {
     switch (mu) {
-        case 1: return run_pcg<1, MAXB>;
-        case 2: return run_pcg<2, MAXB>;
-        case 4: return run_pcg<4, MAXB>;
-        case 8: return run_pcg<8, MAXB>;
+        case 1: return run_pcg<1, MAXB, SF>;
+        case 2: return run_pcg<2, MAXB, SF>;
     }
     return nullptr;
 }
-PcgFn pick(int mu, int maxb) {
-    if (maxb <= 1) return pick_mu<1>(mu);
-    if (maxb <= 4) return pick_mu<4>(mu);
-    if (maxb <= 8) return pick_mu<8>(mu);
-    if (maxb <= 32) return pick_mu<32>(mu);
+template <int SF>
+PcgFn pick_b(int mu, int maxb) {
+    if (maxb <= 1) return pick_mu<1, SF>(mu);
+    if (maxb <= 4) return pick_mu<4, SF>(mu);
+    if (maxb <= 8) return pick_mu<8, SF>(mu);
+    if (maxb <= 32) return pick_mu<32, SF>(mu);
     return nullptr;
+}
+PcgFn pick(int mu, int maxb, int sf) {
+    switch (sf) {
+        case S_BSR_REAL: return pick_b<S_BSR_REAL>(mu, maxb);
+        case S_BSR_CPLX: return pick_b<S_BSR_CPLX>(mu, maxb);
+    }
+    return pick_b<S_CSR>(mu, maxb);
 }
 
 }  // namespace
@@ -822,7 +844,8 @@ int kmsd_metric_s::solve(const double2 *B, double2 *Y, int64_t b, double rtol, d
     const auto start = std::chrono::steady_clock::now();
     if (ensure(b)) return KMSD_ECUDA;
     const RowMap mp = make_map((int)b, kThreads);
-    PcgFn fn = pick(mu_for(mp), nblocks ? maxb : 1);
+    const int sf = S->bsr_nb > 0 ? (S->bsr64().im ? S_BSR_CPLX : S_BSR_REAL) : S_CSR;
+    PcgFn fn = pick(mu_for(mp), nblocks ? maxb : 1, sf);
     if (!fn) return fail(KMSD_EINVAL, "unsupported metric block size / column count");
     const bool sync = status == nullptr;
     // Synchronous calls use a private status word and report.

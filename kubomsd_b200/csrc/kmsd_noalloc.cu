@@ -190,8 +190,6 @@ int dispatch(kmsd_engine_s *e, const double2 *B, double *mu, int64_t b, int64_t 
     switch (mu_for(mp)) {
         case 1: return run<T, 1>(e, B, mu, b, length, center, half, doubling, s);
         case 2: return run<T, 2>(e, B, mu, b, length, center, half, doubling, s);
-        case 4: return run<T, 4>(e, B, mu, b, length, center, half, doubling, s);
-        case 8: return run<T, 8>(e, B, mu, b, length, center, half, doubling, s);
     }
     return fail(KMSD_EINVAL, "too many columns for one engine call");
 }

@@ -165,8 +165,6 @@ int launch_step_h(E *e, StepArgs<T> &a, cudaStream_t s) {
     switch (mu_for(a.mp)) {
         case 1: return launch_step_mu<T, 1, MODE, HSRC, IV>(e, a, s);
         case 2: return launch_step_mu<T, 2, MODE, HSRC, IV>(e, a, s);
-        case 4: return launch_step_mu<T, 4, MODE, HSRC, IV>(e, a, s);
-        case 8: return launch_step_mu<T, 8, MODE, HSRC, IV>(e, a, s);
     }
     return fail(KMSD_EINVAL, "too many columns for one engine call");
 }
