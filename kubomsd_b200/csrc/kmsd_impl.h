@@ -111,6 +111,7 @@ struct kmsd_metric_s {
     int64_t *foff = nullptr;  // device
     double2 *factors = nullptr;
     int maxb = 1;
+    int ub = 0;               // uniform block size (block i = rows [i*ub, (i+1)*ub)), else 0
     bool identity = false;
     int adaptive = 0, interval = 32;
     double gap_ratio = .1;

@@ -113,8 +113,12 @@ template <int MU, bool CPLX>
 __device__ __forceinline__ void gather_block_row(const BsrView<double> &A, const double2 *X, int64_t I, int U,
                                                  int G, int lane, Pk<double> (&acc)[4][MU]) {
     const int k0 = __ldg(A.bptr + I), k1 = __ldg(A.bptr + I + 1);
+    // the next block's column index is loaded one block ahead, so each
+    // block's gathers wait for one memory round trip, not two
+    int Jn = k0 < k1 ? __ldg(A.bidx + k0) : 0;
     for (int k = k0; k < k1; ++k) {
-        const int J = __ldg(A.bidx + k);
+        const int J = Jn;
+        if (k + 1 < k1) Jn = __ldg(A.bidx + k + 1);
         Pk<double> x[MU][4];
 #pragma unroll
         for (int m = 0; m < MU; ++m) {

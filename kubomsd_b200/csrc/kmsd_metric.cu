@@ -60,6 +60,7 @@ struct Pre {
     const int *bstart;
     const int64_t *foff;
     const double2 *factors;
+    int ub;  // uniform block size, or 0: rows and factors are then found without lookups
 };
 
 __device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
@@ -77,6 +78,9 @@ __device__ __forceinline__ void block_rows(const Pre &P, int64_t bi, int64_t &r0
     if (MAXB == 1) {
         r0 = bi;
         m = 1;
+    } else if (P.ub) {
+        r0 = bi * P.ub;
+        m = P.ub;
     } else {
         r0 = P.bstart[bi];
         m = P.bstart[bi + 1] - (int)r0;
@@ -93,7 +97,7 @@ __device__ __forceinline__ void precond(const Pre &P, int64_t bi, int64_t r0, in
         z[0] = make_double2(r[0].x / d, r[0].y / d);
         return;
     }
-    const double2 *L = P.factors + P.foff[bi];
+    const double2 *L = P.factors + (P.ub ? bi * P.ub * P.ub : P.foff[bi]);
     if constexpr (MAXB > 8) {
         // Large blocks: plain loops (registers spill to local memory).
         for (int i = 0; i < m; ++i) {
@@ -150,6 +154,14 @@ __device__ __forceinline__ void precond(const Pre &P, int64_t bi, int64_t r0, in
     }
 }
 
+// CTAs per SM the block kernels (init, update, restart) are compiled for
+// when blocks have at most four rows; they are latency bound, so occupancy
+// is traded against a few bytes of register spill.
+#ifndef KMSD_PCG_MINB4
+#define KMSD_PCG_MINB4 4
+#endif
+#define KMSD_PCG_MINB(maxb) ((maxb) <= 4 ? KMSD_PCG_MINB4 : 1)
+
 #define ZERO_ACC(acc)                                   \
     _Pragma("unroll") for (int m_ = 0; m_ < MU; ++m_) { \
         acc[m_][0] = make_double2(0., 0.);              \
@@ -188,7 +200,7 @@ __global__ void __launch_bounds__(256) pcg_scale_kernel(const double2 *B, int64_
 
 // ---- init: q = B/safe, r = q, y = 0, z = M^-1 r; sums |q|^2 and Re<r,z>
 template <int MU, int MAXB>
-__global__ void __launch_bounds__(256) pcg_init_kernel(const double2 *B, double2 *q, double2 *y, double2 *r,
+__global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB)) pcg_init_kernel(const double2 *B, double2 *q, double2 *y, double2 *r,
                                                        double2 *z, Pre P, int64_t nb, RowMap mp, ColPtr c,
                                                        double rtol, double atol, double2 *partial, Ticket *tk) {
     extern __shared__ double2 smem[];
@@ -347,7 +359,7 @@ __global__ void __launch_bounds__(256) pcg_spmv_kernel(CsrView<double> S, BsrVie
 
 // ---- y += alpha p, r -= alpha sp, z = M^-1 r; sums |r|^2, Re<r,z>
 template <int MU, int MAXB>
-__global__ void __launch_bounds__(256) pcg_update_kernel(double2 *y, double2 *r, double2 *z, const double2 *p,
+__global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB)) pcg_update_kernel(double2 *y, double2 *r, double2 *z, const double2 *p,
                                                          const double2 *sp, Pre P, int64_t nb, RowMap mp, ColPtr c,
                                                          int refresh, int adaptive, double2 *partial, Ticket *tk) {
     if (*(volatile int *)c.flags) return;
@@ -495,7 +507,7 @@ __global__ void __launch_bounds__(256) pcg_true_residual_kernel(CsrView<double> 
 
 // ---- after a check: r <- t on restarted columns, z = M^-1 r, beta
 template <int MU, int MAXB>
-__global__ void __launch_bounds__(256) pcg_restart_kernel(double2 *r, double2 *z, const double2 *t, Pre P,
+__global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB)) pcg_restart_kernel(double2 *r, double2 *z, const double2 *t, Pre P,
                                                           int64_t nb, RowMap mp, ColPtr c, double2 *partial,
                                                           Ticket *tk) {
     if (*(volatile int *)c.flags || !*(volatile int *)(c.flags + 1)) return;
@@ -746,7 +758,7 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
     if (M->red.ensure(grid_mx, (int)b)) return KMSD_ECUDA;
     const size_t sm = reduce_smem(mp, 1);
     ColPtr c = col_ptr(M->cols.p, b);
-    Pre P{M->diag, M->bstart, M->foff, M->factors};
+    Pre P{M->diag, M->bstart, M->foff, M->factors, M->ub};
     const CsrView<double> S = M->S->view64();
     Counters *cnt = M->dcount.as<Counters>();
     double2 *q = M->q.as<double2>(), *y = M->y.as<double2>(), *r = M->r.as<double2>(), *z = M->z.as<double2>(),
@@ -990,6 +1002,15 @@ int kmsd_metric_create(kmsd_csr s, const double *diag, int64_t nblocks, const in
     M->n = n;
     M->nblocks = nblocks;
     M->maxb = maxb;
+    // Uniform partition with factors packed in block order (atom blocks of
+    // one size): the kernels then compute rows and factor offsets directly.
+    if (nblocks > 0) {
+        bool uni = n % nblocks == 0;
+        const int64_t m0 = uni ? n / nblocks : 0;
+        for (int64_t i = 0; i < nblocks && uni; ++i)
+            uni = block_start[i] == i * m0 && factor_offset[i] == i * m0 * m0;
+        M->ub = uni ? (int)m0 : 0;
+    }
     std::vector<double> zinv(n);
     for (int64_t i = 0; i < n; ++i) zinv[i] = 1. / std::sqrt(diag[i]);
     bool unit_diag = true;
