@@ -38,9 +38,11 @@ METRIC = "orbital·moment·vec/s mixed vs FP64 @MSD relerr≤1e-4; HBM GB/s; p50
 UNIT = "orbital·moment·vec/s"
 BOUNDS = (-9.2, 9.2)
 FALLBACK_HBM_GBS = 6650.0
-# dram bytes per launch of the dominant kernel from the ncu capture summarised in
-# profiles/cheb_step_doubling_f32_honeycomb.md (None until captured).
-NCU_TRAFFIC_PER_LAUNCH = None
+# dram bytes (read + write) per launch of the dominant kernel for the default
+# workload: an ncu capture of one step-kernel launch on 524,288 sites x 64
+# complex64 columns read 553.9 MB and wrote 234.0 MB; traffic grows with the
+# rows, so a 4,194,304-site launch moves (553.9 + 234.0) MB x 8.
+NCU_TRAFFIC_PER_LAUNCH = (553.9e6 + 234.0e6) * 8
 
 
 def parse():
@@ -341,8 +343,10 @@ def main():
     avg_launch_s = (ms_step / 1e3) / launches_per_step
     achieved = bytes_per_launch / avg_launch_s / 1e9
     peak, peak_src = peaks()
+    default_shape = (args.lx, args.ly, R, args.precision, args.method) == (2048, 1024, 64, "mixed", "doubling")
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": NCU_TRAFFIC_PER_LAUNCH, "peak_source": peak_src, "kernel": "cheb_step_kernel",
+            "traffic": NCU_TRAFFIC_PER_LAUNCH if default_shape else None, "peak_source": peak_src,
+            "kernel": "cheb_step_kernel",
             "algorithmic_bytes_per_launch": bytes_per_launch, "launches_per_step": launches_per_step,
             "bytes_per_omv": bytes_per_launch / (n * R * (2 if args.method == "doubling" else 1)),
             "timing": "step time / launches per step (includes the 3 small set-up kernels of each step)"}
