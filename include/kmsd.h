@@ -159,6 +159,18 @@ int kmsd_metric_solve(kmsd_metric m, const void *b_in, void *y_out, int64_t b,
                       double rtol, double atol, int maxiter,
                       kmsd_solve_report *report, void *stream);
 
+/* Declare S block-diagonal over the row ranges [row_offsets[s],
+ * row_offsets[s+1]), s < nseg (row_offsets[0] = 0, row_offsets[nseg] = n): a
+ * later kmsd_metric_solve then runs one CG per (segment, column), each with
+ * the reference's per-column semantics (thresholds, breakdown, refresh,
+ * acceptance), all segments in the same launches.  This solves the metric
+ * systems of many independent instances (a ragged batch) at once.  The
+ * report arrays then hold nseg * b entries, segment-major.  Fails with
+ * KMSD_EINVAL when S couples two segments or a block-Jacobi block crosses a
+ * boundary; nseg <= 1 restores the single system.  No counterpart in the
+ * reference, which solves one system per metric. */
+int kmsd_metric_set_segments(kmsd_metric m, int64_t nseg, const int64_t *row_offsets);
+
 /* out = D^-1/2 p(W) xi with W = (D^-1/2 S D^-1/2 - center)/half and p the
  * Chebyshev series `coeff` (Clenshaw).  Replaces Metric::sample
  * (cpp/native.cpp:453-479). */
@@ -277,6 +289,18 @@ typedef struct kmsd_batch_s *kmsd_batch;
 int kmsd_batch_create(int64_t ninst, const kmsd_csr *h, int precision,
                       int64_t tile_rows, kmsd_batch *out);
 void kmsd_batch_destroy(kmsd_batch bt);
+
+/* Make the batch nonorthogonal: `h` is the block-diagonal H of all
+ * instances (any storage form; 4x4 blocks pay for atom-block models) and `m`
+ * a metric over the block-diagonal S with its preconditioner; the batch
+ * declares m's segments to be its instances (kmsd_metric_set_segments).
+ * kmsd_batch_moments then computes, per instance, mu_k = Re<S B, T_k(H~) B>
+ * with T_k advanced by S^-1 H through one segmented PCG per step, in FP64,
+ * with direct moments (KMSD_MOMENTS_DOUBLING is rejected) and without a
+ * CUDA graph (the PCG loop stops on a polled device flag).  The handles stay
+ * owned by the caller and must outlive the batch's use of them. */
+int kmsd_batch_attach_metric(kmsd_batch bt, kmsd_csr h, kmsd_metric m, double rtol,
+                             double atol, int maxiter);
 
 /* Row offsets of the instances in the concatenated vector block (ninst+1
  * values, host). */

@@ -55,6 +55,7 @@ SIGNATURES = {
     "kmsd_metric_create": (C.c_int, [P, PD, I64, PI64, PI64, PD, PD, C.POINTER(P)]),
     "kmsd_metric_destroy": (None, [P]),
     "kmsd_metric_set_residual_policy": (C.c_int, [P, C.c_int, C.c_int, D]),
+    "kmsd_metric_set_segments": (C.c_int, [P, I64, PI64]),
     "kmsd_metric_solve": (C.c_int, [P, P, P, I64, D, D, C.c_int, C.POINTER(SolveReport), P]),
     "kmsd_metric_sample": (C.c_int, [P, P, P, I64, PD, I64, D, D, P]),
     "kmsd_metric_stats_get": (C.c_int, [P, C.POINTER(MetricStats)]),
@@ -73,6 +74,7 @@ SIGNATURES = {
     "kmsd_engine_inner": (C.c_int, [P, P, P, P, I64, P]),
     "kmsd_column_dot": (C.c_int, [P, P, I64, I64, P, P]),
     "kmsd_batch_create": (C.c_int, [I64, C.POINTER(P), C.c_int, I64, C.POINTER(P)]),
+    "kmsd_batch_attach_metric": (C.c_int, [P, P, P, D, D, C.c_int]),
     "kmsd_batch_destroy": (None, [P]),
     "kmsd_batch_rows": (C.c_int, [P, PI64]),
     "kmsd_batch_moments": (C.c_int, [P, P, PD, I64, I64, PD, PD, C.c_int, C.c_int, P]),

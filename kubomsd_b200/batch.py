@@ -1,8 +1,8 @@
 """Ragged batches of independent Hamiltonians (the batching form).
 
-`B200Batch` wraps `kmsd_batch_*` (include/kmsd.h): many orthogonal-basis
-Hamiltonians of uneven size, such as disorder realisations, concatenated
-block-diagonally on the device.  One kernel per Chebyshev step covers all of
+`B200Batch` wraps `kmsd_batch_*` (include/kmsd.h): many Hamiltonians of
+uneven size, such as disorder realisations, concatenated block-diagonally on
+the device (with their overlap matrices for a nonorthogonal basis).  One kernel per Chebyshev step covers all of
 them, with per-instance spectral windows and per-instance moment reductions.
 The whole step sequence is captured into a CUDA graph and replayed.  `tune()`
 picks the row-tile size by timing.  The moments of every instance equal those
@@ -19,9 +19,24 @@ from .native import DeviceCSR, _check, _ptr, _stream, _torch
 
 
 class B200Batch:
-    def __init__(self, hamiltonians, precision="mixed", tile_rows=0):
+    """Moments of many independent instances in one call.
+
+    Orthogonal instances (`overlaps=None`): mixed or FP64, one step kernel per
+    Chebyshev step over all instances, replayed from a CUDA graph.
+    Nonorthogonal instances (`overlaps` = one S per instance, `blocks` = the
+    block-Jacobi factors (a, b, L) of each instance in its own row numbering,
+    or None for the diagonal preconditioner): FP64, direct moments
+    mu_k = Re<S B, T_k> per instance, S^-1 applied by one segmented PCG per
+    step over all instances (one CG per instance and column, as the reference
+    solves each instance).
+    """
+
+    def __init__(self, hamiltonians, precision="mixed", tile_rows=0, overlaps=None, blocks=None, rtol=1e-10,
+                 atol=0., maxiter=1000, residual_policy="fixed", check_interval=32, gap_ratio=.1):
         self.lib = _abi.require_library()
         torch = _torch()
+        if overlaps is not None and precision != "fp64":
+            raise ValueError("a batch of nonorthogonal instances runs in FP64 (precision='fp64')")
         self.parts = [DeviceCSR(H, self.lib) for H in hamiltonians]
         self.ninst = len(self.parts)
         handles = (C.c_void_p * self.ninst)(*[p.handle.value for p in self.parts])
@@ -35,7 +50,30 @@ class B200Batch:
         _check(self.lib, self.lib.kmsd_batch_rows(h, off.ctypes.data_as(C.POINTER(C.c_int64))))
         self.offsets = off
         self.n = int(off[-1])
+        self.metric = None
+        if overlaps is not None:
+            self._attach_metric(hamiltonians, overlaps, blocks, rtol, atol, maxiter, residual_policy, check_interval,
+                                gap_ratio)
         del torch
+
+    def _attach_metric(self, hamiltonians, overlaps, blocks, rtol, atol, maxiter, policy, interval, gap):
+        import scipy.sparse as sp
+        from types import SimpleNamespace
+        from .native import B200Metric
+        if len(overlaps) != self.ninst:
+            raise ValueError("one overlap matrix per instance is required")
+        Hg = sp.block_diag([sp.csr_matrix(H) for H in hamiltonians], format="csr")
+        Sg = sp.block_diag([sp.csr_matrix(S) for S in overlaps], format="csr")
+        gblocks = []
+        if blocks is not None:
+            for off, bl in zip(self.offsets[:-1], blocks):
+                gblocks += [(int(off) + a, int(off) + b, L) for a, b, L in bl]
+        cfg = SimpleNamespace(metric_solver="pcg", metric_residual_policy=policy, metric_check_interval=interval,
+                              metric_gap_ratio=gap)
+        self.hglobal = DeviceCSR(Hg, self.lib)
+        self.metric = B200Metric(Sg, Sg.diagonal().real.copy(), gblocks, cfg)
+        _check(self.lib, self.lib.kmsd_batch_attach_metric(self.handle, self.hglobal.handle, self.metric.handle,
+                                                           float(rtol), float(atol), int(maxiter)))
 
     def concat(self, blocks):
         """Concatenate per-instance (N_i, b) blocks into one device block."""
@@ -57,6 +95,8 @@ class B200Batch:
         mu = getattr(self, "_mu", None)
         if mu is None or mu.shape != (self.ninst, length, b):
             mu = self._mu = torch.empty((self.ninst, length, b), dtype=torch.float64, device="cuda")
+        if self.metric is not None:
+            doubling = False  # the product identity needs S = I
         flags = _abi.KMSD_MOMENTS_DOUBLING if doubling else _abi.KMSD_MOMENTS_DIRECT
         rc = self.lib.kmsd_batch_moments(self.handle, _ptr(B), C.cast(C.c_void_p(mu.data_ptr()),
                                                                       C.POINTER(C.c_double)),
@@ -75,6 +115,8 @@ class B200Batch:
         h = np.ascontiguousarray(np.broadcast_to(np.asarray(halves, float), (self.ninst,)))
         mu = torch.empty((self.ninst, length, b), dtype=torch.float64, device="cuda")
         chosen = C.c_int64()
+        if self.metric is not None:
+            doubling = False
         flags = _abi.KMSD_MOMENTS_DOUBLING if doubling else _abi.KMSD_MOMENTS_DIRECT
         rc = self.lib.kmsd_batch_tune(self.handle, _ptr(B), C.cast(C.c_void_p(mu.data_ptr()), C.POINTER(C.c_double)),
                                       b, int(length), c.ctypes.data_as(C.POINTER(C.c_double)),

@@ -11,6 +11,7 @@
 // calls with the same buffers and shape.  `kmsd_batch_tune` times candidate
 // tile sizes and keeps the fastest.
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <cstring>
 #include <map>
@@ -46,6 +47,7 @@ template <class T> struct BatchArgs {
     const V *curr, *prev;
     V *next;
     const V *bra;
+    const V *hx;  // HSRC_SOLVED: the operator already applied (S^-1 H T_k)
     int first;
     double2 *partial;  // [ntiles][ncol] (x2 for doubling)
 };
@@ -83,8 +85,17 @@ __global__ void __launch_bounds__(256) batch_step_kernel(const BatchArgs<T> a) {
                     po[m] = a.first ? pk_zero<T>() : ld(a.prev + o);
                 }
             }
-            if (HSRC == HSRC_ELL) gather_row_ell<T, MU>(a.E, a.curr, row, mp.U, mp.G, lane, h);
-            else gather_row<T, MU>(a.H, a.curr, row, mp.U, mp.G, lane, h);
+            if (HSRC == HSRC_SOLVED) {
+#pragma unroll
+                for (int m = 0; m < MU; ++m) {
+                    const int u = lane + m * mp.G;
+                    if (u < mp.U) h[m] = ld(a.hx + (size_t)row * mp.U + u);
+                }
+            } else if (HSRC == HSRC_ELL) {
+                gather_row_ell<T, MU>(a.E, a.curr, row, mp.U, mp.G, lane, h);
+            } else {
+                gather_row<T, MU>(a.H, a.curr, row, mp.U, mp.G, lane, h);
+            }
 #pragma unroll
             for (int m = 0; m < MU; ++m) {
                 const int u = lane + m * mp.G;
@@ -118,6 +129,33 @@ __global__ void __launch_bounds__(256) batch_step_kernel(const BatchArgs<T> a) {
         cta_column_sums_at<MU, C>(acc0, mp, ncol, smem, a.partial + (size_t)tile * ncol * 2);
         if (MODE == MODE_DOUBLING)
             cta_column_sums_at<MU, C>(acc1, mp, ncol, smem, a.partial + (size_t)tile * ncol * 2 + ncol);
+    }
+}
+
+// Per tile: Re sum_rows conj(bra) x per column (mu_0 = Re<S B, B> of the
+// nonorthogonal path), laid out as batch_step_kernel's MODE_DIRECT partials.
+template <int MU>
+__global__ void __launch_bounds__(256) batch_dot_kernel(const BatchArgs<double> a, const double2 *x) {
+    extern __shared__ double2 smem[];
+    const RowMap mp = a.mp;
+    const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    const int ncol = mp.U;
+    for (int64_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+        double2 acc[MU][1];
+#pragma unroll
+        for (int m = 0; m < MU; ++m) acc[m][0] = make_double2(0., 0.);
+        for (int64_t row = a.tr0[tile] + g; row < a.tr1[tile]; row += mp.gpc) {
+#pragma unroll
+            for (int m = 0; m < MU; ++m) {
+                const int u = lane + m * mp.G;
+                if (u < mp.U) {
+                    const size_t o = (size_t)row * mp.U + u;
+                    const double2 br = a.bra[o], xv = x[o];
+                    acc[m][0].x += br.x * xv.x + br.y * xv.y;
+                }
+            }
+        }
+        cta_column_sums_at<MU, 1>(acc, mp, ncol, smem, a.partial + (size_t)tile * ncol * 2);
     }
 }
 
@@ -174,6 +212,13 @@ struct kmsd_batch_s {
     std::map<std::tuple<const void *, const void *, int64_t, int64_t, int, int64_t>, cudaGraphExec_t> graphs;
     int64_t kernels_per_graph = 0;
     cudaStream_t cap = nullptr;  // capture stream
+    // Nonorthogonal instances: the block-diagonal H (any storage form) and a
+    // metric over the block-diagonal S, segmented by instance.
+    kmsd_csr_s *gh = nullptr;
+    kmsd_metric_s *gm = nullptr;
+    double rtol = 1e-10, atol = 0.;
+    int maxiter = 1000;
+    DevBuf hx, t1, status, report;
 };
 
 namespace {
@@ -296,6 +341,94 @@ int record(kmsd_batch_s *bt, const double2 *B, double *mu, int64_t b, int64_t le
     return KMSD_OK;
 }
 
+template <class T, int MU, int MODE, int HSRC>
+void launch_tiles(const BatchArgs<T> &a, int64_t ntiles, cudaStream_t s) {
+    const size_t sm = reduce_smem(a.mp, Unit<T>::C);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_step_kernel<T, MU, MODE, HSRC>, kThreads, sm) !=
+        cudaSuccess)
+        per_sm = 1;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)sm_count() * std::max(per_sm, 1)));
+    batch_step_kernel<T, MU, MODE, HSRC><<<grid, kThreads, sm, s>>>(a);
+}
+
+// Nonorthogonal batch (FP64): per step one SpMM of the block-diagonal H, one
+// segmented PCG over every instance's S (one CG per instance and column),
+// and one tile step kernel on the solved operand; mu_k = Re<S B, T_k> per
+// instance (Engine::moments, cpp/native.cpp:590-609, for each instance).
+template <int MU>
+int run_general(kmsd_batch_s *bt, const double2 *B, double *mu, int64_t b, int64_t length, cudaStream_t s) {
+    const int64_t n = bt->n;
+    const RowMap mp = make_map((int)b, kThreads);
+    const int ncol = (int)b;
+    const size_t vb = (size_t)n * b * sizeof(double2);
+    if (bt->ta.ensure(vb) || bt->tb.ensure(vb) || bt->bra.ensure(vb) || bt->hx.ensure(vb) || bt->t1.ensure(vb) ||
+        bt->partial.ensure((size_t)bt->tiles.ntiles * ncol * 2 * sizeof(double2) + 256) ||
+        bt->status.ensure(4 * sizeof(int)) || bt->report.ensure(sizeof(FailReportFull)))
+        return KMSD_ECUDA;
+    int *status = bt->status.as<int>();
+    KMSD_CUDA(cudaMemsetAsync(status, 0, 4 * sizeof(int), s));
+    double2 *ta = bt->ta.as<double2>(), *tb = bt->tb.as<double2>(), *sb = bt->bra.as<double2>();
+    double2 *hx = bt->hx.as<double2>(), *t1 = bt->t1.as<double2>();
+    BatchArgs<double> a;
+    std::memset(&a, 0, sizeof(a));
+    a.mp = mp;
+    a.tseg = bt->tiles.seg;
+    a.tr0 = bt->tiles.r0;
+    a.tr1 = bt->tiles.r1;
+    a.ntiles = bt->tiles.ntiles;
+    a.center = bt->dcenter.as<double>();
+    a.half = bt->dhalf.as<double>();
+    a.partial = bt->partial.as<double2>();
+    a.bra = sb;
+    a.hx = hx;
+    int rc = spmm64(bt->gm->S, B, sb, b, s);  // S B, the bra of every moment
+    if (rc) return rc;
+    {
+        const size_t sm = reduce_smem(mp, 1);
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(a.ntiles, (int64_t)sm_count() * 4));
+        batch_dot_kernel<MU><<<grid, kThreads, sm, s>>>(a, B);
+        batch_finalize_kernel<MODE_DIRECT><<<(int)bt->ninst, 128, 0, s>>>(a.partial, bt->tiles.seg_tile0, ncol,
+                                                                          (int)b, mu, length, 0);
+        count_launch(2);
+    }
+    const double2 *curr = B, *prev = nullptr;
+    for (int64_t k = 1; k < length; ++k) {
+        double2 *next = k == 1 ? ta : k == 2 ? tb : const_cast<double2 *>(prev);
+        if ((rc = spmm64(bt->gh, curr, t1, b, s))) return rc;
+        if ((rc = bt->gm->solve(t1, hx, b, bt->rtol, bt->atol, bt->maxiter, nullptr, s, status, bt->report.p)))
+            return rc;
+        a.curr = curr;
+        a.prev = prev;
+        a.next = next;
+        a.first = k == 1;
+        launch_tiles<double, MU, MODE_DIRECT, HSRC_SOLVED>(a, a.ntiles, s);
+        batch_finalize_kernel<MODE_DIRECT><<<(int)bt->ninst, 128, 0, s>>>(a.partial, bt->tiles.seg_tile0, ncol,
+                                                                          (int)b, mu, length, k);
+        count_launch(2);
+        prev = curr;
+        curr = next;
+    }
+    KMSD_CUDA(cudaGetLastError());
+    // a failed solve of any instance fails the call with the reference's message
+    int st[4];
+    KMSD_CUDA(cudaMemcpyAsync(st, status, sizeof(st), cudaMemcpyDeviceToHost, s));
+    KMSD_CUDA(cudaStreamSynchronize(s));
+    if (st[0] != 0) {
+        FailReportFull fr;
+        KMSD_CUDA(cudaMemcpy(&fr, bt->report.p, sizeof(fr), cudaMemcpyDeviceToHost));
+        switch (fr.head.reason) {
+            case 3: return fail(KMSD_EINVAL, "metric RHS must be finite");
+            case 2:
+                return fail(KMSD_EMETRIC,
+                            "S solve solution is nonfinite or not representable in complex128 after rescaling");
+            case 1: return fail(KMSD_EMETRIC, "PCG non-positive/complex curvature breakdown");
+            default: return fail(KMSD_EMETRIC, "S solve failed true-residual acceptance");
+        }
+    }
+    return KMSD_OK;
+}
+
 template <class T>
 int run_batch(kmsd_batch_s *bt, const double2 *B, double *mu, int64_t b, int64_t length, bool doubling,
               cudaStream_t s, bool use_graph) {
@@ -385,6 +518,14 @@ int batch_call(kmsd_batch_s *bt, const void *b_in, double *mu, int64_t b, int64_
         KMSD_CUDA(cudaStreamSynchronize(s));
         bt->last_center.assign(center, center + bt->ninst);
         bt->last_half.assign(half, half + bt->ninst);
+    }
+    if (bt->gm) {
+        if (doubling) return fail(KMSD_EINVAL, "moment doubling needs an orthogonal basis (S = I)");
+        const RowMap mp = make_map((int)b, kThreads);
+        const int m = mu_for(mp);
+        if (!m || b > 256) return fail(KMSD_EINVAL, "too many columns for one batch call");
+        return m == 1 ? run_general<1>(bt, static_cast<const double2 *>(b_in), mu, b, length, s)
+                      : run_general<2>(bt, static_cast<const double2 *>(b_in), mu, b, length, s);
     }
     int rc = bt->precision == KMSD_MIXED
                  ? run_batch<float>(bt, static_cast<const double2 *>(b_in), mu, b, length, doubling, s, use_graph)
@@ -515,8 +656,27 @@ void kmsd_batch_destroy(kmsd_batch bt) {
                     (void *)G.ell_im32})
         cudaFree(p);
     G = kmsd_csr_s();
-    for (DevBuf *d : {&bt->dcenter, &bt->dhalf, &bt->ta, &bt->tb, &bt->bra, &bt->partial, &bt->tilemem}) d->release();
+    for (DevBuf *d : {&bt->dcenter, &bt->dhalf, &bt->ta, &bt->tb, &bt->bra, &bt->partial, &bt->tilemem, &bt->hx,
+                      &bt->t1, &bt->status, &bt->report})
+        d->release();
     delete bt;
+}
+
+int kmsd_batch_attach_metric(kmsd_batch bt, kmsd_csr h, kmsd_metric m, double rtol, double atol, int maxiter) {
+    if (!bt || !h || !m) return fail(KMSD_EINVAL, "invalid batch metric");
+    if (h->n != bt->n || m->n != bt->n)
+        return fail(KMSD_EINVAL, "the block-diagonal H and S must have the batch's rows");
+    if (bt->precision != KMSD_FP64) return fail(KMSD_EINVAL, "a batch with a metric runs in FP64");
+    if (!(rtol >= 0) || !(atol >= 0) || !std::isfinite(rtol) || !std::isfinite(atol) || maxiter < 1)
+        return fail(KMSD_EINVAL, "invalid metric RHS shape/tolerances");
+    const int rc = kmsd_metric_set_segments(m, bt->ninst, bt->row_off.data());
+    if (rc) return rc;
+    bt->gh = h;
+    bt->gm = m;
+    bt->rtol = rtol;
+    bt->atol = atol;
+    bt->maxiter = maxiter;
+    return KMSD_OK;
 }
 
 int kmsd_batch_rows(kmsd_batch bt, int64_t *offsets) {

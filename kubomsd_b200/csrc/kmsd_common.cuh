@@ -320,40 +320,57 @@ __device__ __forceinline__ bool arrive_last(Ticket *t, unsigned expected) {
     return is_last;
 }
 
-__device__ __forceinline__ bool tree_column_sums(double2 *partial, int ncol, Ticket *tk, double2 *smem,
-                                                 double2 *out) {
-    const int grid = gridDim.x;
-    const int ngroups = (grid + kTreeFan - 1) / kTreeFan;
+// The same over the consecutive CTAs [c0, c0 + nct) of one range (a segment
+// of a segmented solve), this CTA being c0 + lc: tickets tks[0] (root) and
+// tks[1 + group], level-2 rows level2[group * ncol].  Returns true in the CTA
+// that holds the range's totals in out.
+__device__ __forceinline__ bool range_column_sums(double2 *partial, int ncol, int c0, int nct, int lc, Ticket *tks,
+                                                  double2 *level2, double2 *smem, double2 *out) {
+    const int ngroups = (nct + kTreeFan - 1) / kTreeFan;
     if (ngroups == 1) {
-        if (!arrive_last(tk, grid)) return false;
-        final_column_sums(partial, grid, ncol, smem, out);
+        if (!arrive_last(tks, nct)) return false;
+        final_column_sums(partial + (size_t)c0 * ncol, nct, ncol, smem, out);
         return true;
     }
-    const int group = blockIdx.x / kTreeFan, lo = group * kTreeFan, cnt = min(kTreeFan, grid - lo);
-    if (!arrive_last(tk + 1 + group, cnt)) return false;
-    double2 *level2 = partial + (size_t)grid * ncol;
-    final_column_sums(partial + (size_t)lo * ncol, cnt, ncol, smem, level2 + (size_t)group * ncol);
-    if (!arrive_last(tk, ngroups)) return false;
+    const int group = lc / kTreeFan, lo = group * kTreeFan, cnt = min(kTreeFan, nct - lo);
+    if (!arrive_last(tks + 1 + group, cnt)) return false;
+    final_column_sums(partial + (size_t)(c0 + lo) * ncol, cnt, ncol, smem, level2 + (size_t)group * ncol);
+    if (!arrive_last(tks, ngroups)) return false;
     final_column_sums(level2, ngroups, ncol, smem, out);
     return true;
 }
 
-__device__ __forceinline__ bool tree_column_max(double *partial, int ncol, Ticket *tk, double *out) {
-    const int grid = gridDim.x;
-    const int ngroups = (grid + kTreeFan - 1) / kTreeFan;
+__device__ __forceinline__ bool range_column_max(double *partial, int ncol, int c0, int nct, int lc, Ticket *tks,
+                                                 double *level2, double *out) {
+    const int ngroups = (nct + kTreeFan - 1) / kTreeFan;
     if (ngroups == 1) {
-        if (!arrive_last(tk, grid)) return false;
-        final_column_max(partial, grid, ncol, out);
+        if (!arrive_last(tks, nct)) return false;
+        final_column_max(partial + (size_t)c0 * ncol, nct, ncol, out);
         return true;
     }
-    const int group = blockIdx.x / kTreeFan, lo = group * kTreeFan, cnt = min(kTreeFan, grid - lo);
-    if (!arrive_last(tk + 1 + group, cnt)) return false;
-    double *level2 = partial + (size_t)grid * ncol;
-    final_column_max(partial + (size_t)lo * ncol, cnt, ncol, level2 + (size_t)group * ncol);
+    const int group = lc / kTreeFan, lo = group * kTreeFan, cnt = min(kTreeFan, nct - lo);
+    if (!arrive_last(tks + 1 + group, cnt)) return false;
+    final_column_max(partial + (size_t)(c0 + lo) * ncol, cnt, ncol, level2 + (size_t)group * ncol);
     __syncthreads();
-    if (!arrive_last(tk, ngroups)) return false;
+    if (!arrive_last(tks, ngroups)) return false;
     final_column_max(level2, ngroups, ncol, out);
     return true;
+}
+
+// Tickets a range of nct CTAs uses.
+__host__ __device__ inline int range_tickets(int nct) {
+    const int ngroups = (nct + kTreeFan - 1) / kTreeFan;
+    return ngroups == 1 ? 1 : 1 + ngroups;
+}
+
+__device__ __forceinline__ bool tree_column_sums(double2 *partial, int ncol, Ticket *tk, double2 *smem,
+                                                 double2 *out) {
+    return range_column_sums(partial, ncol, 0, gridDim.x, blockIdx.x, tk, partial + (size_t)gridDim.x * ncol, smem,
+                             out);
+}
+
+__device__ __forceinline__ bool tree_column_max(double *partial, int ncol, Ticket *tk, double *out) {
+    return range_column_max(partial, ncol, 0, gridDim.x, blockIdx.x, tk, partial + (size_t)gridDim.x * ncol, out);
 }
 
 // ---------------------------------------------------------------- host errors

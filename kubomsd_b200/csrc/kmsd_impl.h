@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -126,7 +127,25 @@ struct kmsd_metric_s {
     int64_t calls = 0;
     double seconds = 0.;
     kmsd::DevBuf dcount;  // device counters: refreshes, checks, restarts, iters_sum, max_rel(bits)
-    int ensure(int64_t b);
+    // Segments: S is block-diagonal over the row ranges [seg_row0[s],
+    // seg_row0[s+1]), each an independent system with its own CG per column
+    // (nseg <= 1: one system).  Device descriptors per row-group width.
+    struct SegPlan {
+        kmsd::DevBuf mem;
+        int grid = 0, l2rows = 0;
+        int *cta_seg = nullptr, *cta0 = nullptr, *tk0 = nullptr, *l2 = nullptr, *segn = nullptr,
+            *segchk = nullptr;
+        int64_t *row0 = nullptr, *blk0 = nullptr;
+        kmsd::Ticket *tickets = nullptr;
+    };
+    int64_t nseg = 0;
+    std::vector<int64_t> seg_row0, seg_blk0;
+    std::vector<int64_t> bstart_host;  // block-Jacobi partition (host copy)
+    bool seg_aligned4 = false;  // every segment starts on a multiple of 4 rows
+    std::map<int, SegPlan> seg_plans;
+    int seg_plan(int gpc, SegPlan **out);
+    // state_cols: per-column state entries (nseg * b for a segmented solve)
+    int ensure(int64_t b, int64_t state_cols = 0);
     // Batched PCG on device buffers (complex128).  When `report` is null and
     // `status` non-null, the call is asynchronous: a failure is recorded in
     // *status (first failure wins) together with the per-column report in

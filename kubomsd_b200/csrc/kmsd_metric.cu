@@ -167,18 +167,98 @@ __device__ __forceinline__ void precond(const Pre &P, int64_t bi, int64_t r0, in
         acc[m_][0] = make_double2(0., 0.);              \
     }
 
+// ---- segments
+// A segmented solve treats the operator as block-diagonal over nseg row
+// ranges (independent systems: the instances of a ragged batch) and runs one
+// CG per (segment, column), with its column state at index s * b + j.  Every
+// CTA belongs to one segment and walks only that segment's rows, 4x4 block
+// rows and preconditioner blocks; column sums combine per segment (its own
+// tickets and level-2 rows), and a last-segment ticket aggregates the flags
+// that every segment contributes to.  A plain solve is the SEG = false
+// instantiation: one segment over the whole grid.
+struct SegView {
+    int nseg;
+    const int *cta_seg;   // [grid] segment of each CTA
+    const int *cta0;      // [nseg + 1] first CTA of each segment
+    const int64_t *row0;  // [nseg + 1] first row
+    const int64_t *blk0;  // [nseg + 1] first preconditioner block
+    const int *tk0;       // [nseg + 1] first ticket of each segment; tk0[nseg]: the last-segment ticket
+    const int *l2;        // [nseg] first level-2 partial row, counted after the grid's rows
+    int *segn;            // [nseg] active columns of each segment
+    int *segchk;          // [nseg] a true-residual check is due in the segment
+};
+
+// This CTA's segment, its place among the segment's CTAs, and the segment's
+// rows [r0, r1) and preconditioner blocks [b0, b1).
+struct Ctx {
+    int s, lc, nct;
+    int64_t r0, r1, b0, b1;
+};
+
+template <bool SEG>
+__device__ __forceinline__ Ctx seg_ctx(const SegView &sv, int64_t n, int64_t nb) {
+    if constexpr (!SEG) {
+        return Ctx{0, (int)blockIdx.x, (int)gridDim.x, 0, n, 0, nb};
+    } else {
+        const int s = sv.cta_seg[blockIdx.x], c0 = sv.cta0[s];
+        return Ctx{s, (int)blockIdx.x - c0, sv.cta0[s + 1] - c0, sv.row0[s], sv.row0[s + 1], sv.blk0[s],
+                   sv.blk0[s + 1]};
+    }
+}
+
+// True in the CTA that holds this segment's column sums in out.
+template <bool SEG>
+__device__ __forceinline__ bool seg_sums(double2 *partial, int ncol, Ticket *tk, double2 *smem, double2 *out,
+                                         const SegView &sv, const Ctx &x) {
+    if constexpr (!SEG) {
+        return tree_column_sums(partial, ncol, tk, smem, out);
+    } else {
+        return range_column_sums(partial, ncol, (int)blockIdx.x - x.lc, x.nct, x.lc, tk + sv.tk0[x.s],
+                                 partial + (size_t)(gridDim.x + sv.l2[x.s]) * ncol, smem, out);
+    }
+}
+template <bool SEG>
+__device__ __forceinline__ bool seg_max(double *partial, int ncol, Ticket *tk, double *out, const SegView &sv,
+                                        const Ctx &x) {
+    if constexpr (!SEG) {
+        return tree_column_max(partial, ncol, tk, out);
+    } else {
+        return range_column_max(partial, ncol, (int)blockIdx.x - x.lc, x.nct, x.lc, tk + sv.tk0[x.s],
+                                partial + (size_t)(gridDim.x + sv.l2[x.s]) * ncol, out);
+    }
+}
+
+// Called by every CTA that closed its segment: true in the last of them (a
+// plain solve has one segment, so there it is always true).
+template <bool SEG>
+__device__ __forceinline__ bool last_segment(Ticket *tk, const SegView &sv) {
+    if constexpr (!SEG) {
+        return true;
+    } else {
+        return arrive_last(tk + sv.tk0[sv.nseg], sv.nseg);
+    }
+}
+
+// Sum of segn over the segments (thread 0's result), in segment order.
+__device__ __forceinline__ int total_active(const SegView &sv) {
+    int t = 0;
+    for (int s = 0; s < sv.nseg; ++s) t += __ldcg(sv.segn + s);
+    return t;
+}
+
 // ---- column scale: safe_j = max_i max(|Re|,|Im|), nonfinite detection
-template <int MU>
+template <int MU, bool SEG>
 __global__ void __launch_bounds__(256) pcg_scale_kernel(const double2 *B, int64_t n, RowMap mp, ColPtr c,
-                                                        double *partial, Ticket *tk) {
+                                                        double *partial, Ticket *tk, SegView sv) {
     extern __shared__ double2 smem2[];
     double *smem = reinterpret_cast<double *>(smem2);
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    const Ctx x = seg_ctx<SEG>(sv, n, 0);
     double acc[MU][1];
 #pragma unroll
     for (int m = 0; m < MU; ++m) acc[m][0] = 0.;
     bool bad = false;
-    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < n; row += (int64_t)gridDim.x * mp.gpc) {
+    for (int64_t row = x.r0 + (int64_t)x.lc * mp.gpc + g; row < x.r1; row += (int64_t)x.nct * mp.gpc) {
 #pragma unroll
         for (int m = 0; m < MU; ++m) {
             const int u = lane + m * mp.G;
@@ -191,24 +271,27 @@ __global__ void __launch_bounds__(256) pcg_scale_kernel(const double2 *B, int64_
     }
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(c.flags + 2, 1);
     cta_column_max<MU, 1>(acc, mp, mp.U, smem, partial);
-    if (tree_column_max(partial, mp.U, tk, c.safe)) {
+    double *safe = c.safe + (size_t)x.s * mp.U;
+    if (seg_max<SEG>(partial, mp.U, tk, safe, sv, x)) {
         __syncthreads();
         for (int j = threadIdx.x; j < mp.U; j += blockDim.x)
-            if (c.safe[j] == 0.) c.safe[j] = 1.;
+            if (safe[j] == 0.) safe[j] = 1.;
     }
 }
 
 // ---- init: q = B/safe, r = q, y = 0, z = M^-1 r; sums |q|^2 and Re<r,z>
-template <int MU, int MAXB>
-__global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB)) pcg_init_kernel(const double2 *B, double2 *q, double2 *y, double2 *r,
-                                                       double2 *z, Pre P, int64_t nb, RowMap mp, ColPtr c,
-                                                       double rtol, double atol, double2 *partial, Ticket *tk) {
+template <int MU, int MAXB, bool SEG>
+__global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
+    pcg_init_kernel(const double2 *B, double2 *q, double2 *y, double2 *r, double2 *z, Pre P, int64_t nb, RowMap mp,
+                    ColPtr c, double rtol, double atol, double2 *partial, Ticket *tk, SegView sv) {
     extern __shared__ double2 smem[];
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
     const int U = mp.U;
+    const Ctx x = seg_ctx<SEG>(sv, 0, nb);
+    const size_t cs0 = (size_t)x.s * U;
     double2 acc[MU][1];
     ZERO_ACC(acc);
-    for (int64_t bi = (int64_t)blockIdx.x * mp.gpc + g; bi < nb; bi += (int64_t)gridDim.x * mp.gpc) {
+    for (int64_t bi = x.b0 + (int64_t)x.lc * mp.gpc + g; bi < x.b1; bi += (int64_t)x.nct * mp.gpc) {
         int64_t r0;
         int m;
         block_rows<MAXB>(P, bi, r0, m);
@@ -216,7 +299,7 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB)) pcg_init_kernel(cons
         for (int mm = 0; mm < MU; ++mm) {
             const int u = lane + mm * mp.G;
             if (u >= U) continue;
-            const double sf = c.safe[u];
+            const double sf = c.safe[cs0 + u];
             double2 rr[MAXB], zz[MAXB];
 #pragma unroll
             for (int i = 0; i < MAXB; ++i) {
@@ -243,40 +326,60 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB)) pcg_init_kernel(cons
     }
     cta_column_sums<MU, 1>(acc, mp, U, smem, partial);
     __shared__ double2 tot[256];
-    if (tree_column_sums(partial, U, tk, smem, tot)) {
+    if (seg_sums<SEG>(partial, U, tk, smem, tot, sv, x)) {
         __syncthreads();
         const int j = threadIdx.x;
         bool act = false;
         if (j < U) {
+            const size_t cj = cs0 + j;
             const double bn = sqrt(tot[j].x);
-            const double thr = fmax(rtol * bn, atol / c.safe[j]);
+            const double thr = fmax(rtol * bn, atol / c.safe[cj]);
             act = bn > thr;
-            c.bn[j] = bn;
-            c.thr[j] = thr;
-            c.active[j] = act;
-            c.rz[j] = tot[j].y;
-            c.iters[j] = 0;
-            c.brk[j] = 0;
-            c.restart[j] = 0;
-            c.alpha[j] = 0.;
-            c.beta[j] = 0.;
+            c.bn[cj] = bn;
+            c.thr[cj] = thr;
+            c.active[cj] = act;
+            c.rz[cj] = tot[j].y;
+            c.iters[cj] = 0;
+            c.brk[cj] = 0;
+            c.restart[cj] = 0;
+            c.alpha[cj] = 0.;
+            c.beta[cj] = 0.;
         }
         const int nact = __syncthreads_count(act);
-        if (threadIdx.x == 0) {
-            c.flags[0] = nact == 0;  // halt: nothing to iterate
+        if constexpr (SEG) {
+            if (threadIdx.x == 0) {
+                sv.segn[x.s] = nact;
+                sv.segchk[x.s] = 0;
+            }
+        }
+        if (last_segment<SEG>(tk, sv) && threadIdx.x == 0) {
+            const int total = SEG ? total_active(sv) : nact;
+            c.flags[0] = total == 0;  // halt: nothing to iterate
             c.flags[1] = 0;
             c.flags[3] = 0;
-            c.flags[4] = nact;
+            c.flags[4] = total;
         }
     }
 }
 
 // p = active ? z : 0
-__global__ void pcg_pinit_kernel(const double2 *z, double2 *p, int64_t len, int U, ColPtr c) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int j = (int)(i % U);
-        p[i] = c.active[j] ? z[i] : make_double2(0., 0.);
+template <bool SEG>
+__global__ void pcg_pinit_kernel(const double2 *z, double2 *p, int64_t len, RowMap mp, ColPtr c, SegView sv) {
+    if constexpr (!SEG) {
+        const int U = mp.U;
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len;
+             i += (int64_t)gridDim.x * blockDim.x) {
+            const int j = (int)(i % U);
+            p[i] = c.active[j] ? z[i] : make_double2(0., 0.);
+        }
+    } else {
+        const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+        const Ctx x = seg_ctx<SEG>(sv, 0, 0);
+        for (int64_t row = x.r0 + (int64_t)x.lc * mp.gpc + g; row < x.r1; row += (int64_t)x.nct * mp.gpc)
+            for (int u = lane; u < mp.U; u += mp.G) {
+                const size_t o = (size_t)row * mp.U + u;
+                p[o] = c.active[(size_t)x.s * mp.U + u] ? z[o] : make_double2(0., 0.);
+            }
     }
 }
 
@@ -284,14 +387,14 @@ __global__ void pcg_pinit_kernel(const double2 *z, double2 *p, int64_t len, int 
 // complex values.
 enum { S_CSR = 0, S_BSR_REAL = 1, S_BSR_CPLX = 2 };
 
-// Calls f(row, yv) for every row owned by this thread's row group, with
-// yv[m] = (S X)[row, unit lane + m*G], from CSR or from 4x4 blocks (a block
-// row's four rows share every gathered input row).
+// Calls f(row, yv) for every row of rows [x.r0, x.r1) owned by this thread's
+// row group, with yv[m] = (S X)[row, unit lane + m*G], from CSR or from 4x4
+// blocks (a block row's four rows share every gathered input row).
 template <int MU, int SF, class F>
 __device__ __forceinline__ void for_rows_spmv(const CsrView<double> &S, const BsrView<double> &SB, const double2 *X,
-                                              int64_t n, const RowMap &mp, int g, int lane, F &&f) {
+                                              const Ctx &x, const RowMap &mp, int g, int lane, F &&f) {
     if constexpr (SF != S_CSR) {
-        for (int64_t I = (int64_t)blockIdx.x * mp.gpc + g; I < SB.nbrows; I += (int64_t)gridDim.x * mp.gpc) {
+        for (int64_t I = x.r0 / 4 + (int64_t)x.lc * mp.gpc + g; I < x.r1 / 4; I += (int64_t)x.nct * mp.gpc) {
             Pk<double> acc4[4][MU];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
@@ -302,7 +405,7 @@ __device__ __forceinline__ void for_rows_spmv(const CsrView<double> &S, const Bs
             for (int i = 0; i < 4; ++i) f(4 * I + i, acc4[i]);
         }
     } else {
-        for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < n; row += (int64_t)gridDim.x * mp.gpc) {
+        for (int64_t row = x.r0 + (int64_t)x.lc * mp.gpc + g; row < x.r1; row += (int64_t)x.nct * mp.gpc) {
             Pk<double> yv[MU];
 #pragma unroll
             for (int m = 0; m < MU; ++m) yv[m] = pk_zero<double>();
@@ -313,62 +416,75 @@ __device__ __forceinline__ void for_rows_spmv(const CsrView<double> &S, const Bs
 }
 
 // ---- sp = S p, curvature <p, sp>, alpha, breakdown
-template <int MU, int SF>
-__global__ void __launch_bounds__(256) pcg_spmv_kernel(CsrView<double> S, BsrView<double> SB, const double2 *p, double2 *sp,
-                                                       int64_t n, RowMap mp, ColPtr c, double2 *partial,
-                                                       Ticket *tk) {
+template <int MU, int SF, bool SEG>
+__global__ void __launch_bounds__(256)
+    pcg_spmv_kernel(CsrView<double> S, BsrView<double> SB, const double2 *p, double2 *sp, int64_t n, RowMap mp,
+                    ColPtr c, double2 *partial, Ticket *tk, SegView sv) {
     if (*(volatile int *)c.flags) return;
     extern __shared__ double2 smem[];
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    const Ctx x = seg_ctx<SEG>(sv, n, 0);
     double2 acc[MU][1];
     ZERO_ACC(acc);
-    for_rows_spmv<MU, SF>(S, SB, p, n, mp, g, lane, [&](int64_t row, const Pk<double>(&yv)[MU]) {
+    for_rows_spmv<MU, SF>(S, SB, p, x, mp, g, lane, [&](int64_t row, const Pk<double>(&yv)[MU]) {
 #pragma unroll
         for (int m = 0; m < MU; ++m) {
             const int u = lane + m * mp.G;
             if (u < mp.U) {
                 const size_t o = (size_t)row * mp.U + u;
                 sp[o] = make_double2(yv[m].re[0], yv[m].im[0]);
-                const double2 x = p[o];
-                acc[m][0].x += x.x * yv[m].re[0] + x.y * yv[m].im[0];
-                acc[m][0].y += x.x * yv[m].im[0] - x.y * yv[m].re[0];
+                const double2 xv = p[o];
+                acc[m][0].x += xv.x * yv[m].re[0] + xv.y * yv[m].im[0];
+                acc[m][0].y += xv.x * yv[m].im[0] - xv.y * yv[m].re[0];
             }
         }
     });
     cta_column_sums<MU, 1>(acc, mp, mp.U, smem, partial);
     __shared__ double2 tot[256];
-    if (tree_column_sums(partial, mp.U, tk, smem, tot)) {
+    if (seg_sums<SEG>(partial, mp.U, tk, smem, tot, sv, x)) {
         __syncthreads();
         const int j = threadIdx.x;
         bool b = false;
         if (j < mp.U) {
+            const size_t cj = (size_t)x.s * mp.U + j;
             const double cr = tot[j].x, ci = tot[j].y;
-            const bool act = c.active[j];
+            const bool act = c.active[cj];
             if (act && (!(cr > 0.) || !isfinite(cr) || !isfinite(ci) || fabs(ci) > 1e-10 * fmax(fabs(cr), DBL_MIN))) {
-                c.brk[j] = 1;
+                c.brk[cj] = 1;
                 b = true;
             }
-            c.alpha[j] = act ? c.rz[j] / cr : 0.;
+            c.alpha[cj] = act ? c.rz[cj] / cr : 0.;
         }
-        if (__syncthreads_or(b) && threadIdx.x == 0) {
-            c.flags[3] = 1;
-            c.flags[0] = 1;
+        const bool any_brk = __syncthreads_or(b);
+        if constexpr (!SEG) {
+            if (any_brk && threadIdx.x == 0) {
+                c.flags[3] = 1;
+                c.flags[0] = 1;
+            }
+        } else {
+            // Segments halt together, and only once every CTA of this launch
+            // has passed its entry check (a CTA that saw the halt word early
+            // would skip its segment's tickets): the last segment raises it.
+            if (any_brk && threadIdx.x == 0) c.flags[3] = 1;
+            if (last_segment<SEG>(tk, sv) && threadIdx.x == 0 && __ldcg(c.flags + 3)) c.flags[0] = 1;
         }
     }
 }
 
 // ---- y += alpha p, r -= alpha sp, z = M^-1 r; sums |r|^2, Re<r,z>
-template <int MU, int MAXB>
-__global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB)) pcg_update_kernel(double2 *y, double2 *r, double2 *z, const double2 *p,
-                                                         const double2 *sp, Pre P, int64_t nb, RowMap mp, ColPtr c,
-                                                         int refresh, int adaptive, double2 *partial, Ticket *tk) {
+template <int MU, int MAXB, bool SEG>
+__global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
+    pcg_update_kernel(double2 *y, double2 *r, double2 *z, const double2 *p, const double2 *sp, Pre P, int64_t nb,
+                      RowMap mp, ColPtr c, int refresh, int adaptive, double2 *partial, Ticket *tk, SegView sv) {
     if (*(volatile int *)c.flags) return;
     extern __shared__ double2 smem[];
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
     const int U = mp.U;
+    const Ctx x = seg_ctx<SEG>(sv, 0, nb);
+    const size_t cs0 = (size_t)x.s * U;
     double2 acc[MU][1];
     ZERO_ACC(acc);
-    for (int64_t bi = (int64_t)blockIdx.x * mp.gpc + g; bi < nb; bi += (int64_t)gridDim.x * mp.gpc) {
+    for (int64_t bi = x.b0 + (int64_t)x.lc * mp.gpc + g; bi < x.b1; bi += (int64_t)x.nct * mp.gpc) {
         int64_t r0;
         int m;
         block_rows<MAXB>(P, bi, r0, m);
@@ -376,18 +492,18 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB)) pcg_update_kernel(do
         for (int mm = 0; mm < MU; ++mm) {
             const int u = lane + mm * mp.G;
             if (u >= U) continue;
-            const double al = c.alpha[u];
+            const double al = c.alpha[cs0 + u];
             double2 rr[MAXB], zz[MAXB];
 #pragma unroll
             for (int i = 0; i < MAXB; ++i) {
                 if (i < m) {
                     const size_t o = (size_t)(r0 + i) * U + u;
-                    const double2 pv = p[o], sv = sp[o];
+                    const double2 pv = p[o], sv2 = sp[o];
                     double2 yv = y[o], rv = r[o];
                     yv.x += pv.x * al;
                     yv.y += pv.y * al;
-                    rv.x -= sv.x * al;
-                    rv.y -= sv.y * al;
+                    rv.x -= sv2.x * al;
+                    rv.y -= sv2.y * al;
                     y[o] = yv;
                     r[o] = rv;
                     rr[i] = rv;
@@ -406,117 +522,144 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB)) pcg_update_kernel(do
     }
     cta_column_sums<MU, 1>(acc, mp, U, smem, partial);
     __shared__ double2 tot[256];
-    if (tree_column_sums(partial, U, tk, smem, tot)) {
+    if (seg_sums<SEG>(partial, U, tk, smem, tot, sv, x)) {
         __syncthreads();
         const int j = threadIdx.x;
+        const size_t cj = cs0 + j;
         bool cand = false;
         if (j < U) {
-            const int act = c.active[j];
-            c.iters[j] += act;
+            const int act = c.active[cj];
+            c.iters[cj] += act;
             const double rn = sqrt(tot[j].x);
-            c.rn[j] = rn;
-            c.newrz[j] = tot[j].y;
-            cand = act && rn <= c.thr[j];
+            c.rn[cj] = rn;
+            c.newrz[cj] = tot[j].y;
+            cand = act && rn <= c.thr[cj];
         }
         const bool candidate = __syncthreads_or(cand);
         const bool check = refresh || (adaptive && candidate);
         bool act_now = false;
         if (j < U) {
             if (!check) {
-                int act = c.active[j];
-                if (!adaptive) act = act && c.rn[j] > c.thr[j];
-                c.active[j] = act;
-                c.restart[j] = 0;
-                const double rz = c.rz[j], nrz = c.newrz[j];
-                c.beta[j] = act ? nrz / (rz != 0. ? rz : 1.) : 0.;
-                c.rz[j] = nrz;
+                int act = c.active[cj];
+                if (!adaptive) act = act && c.rn[cj] > c.thr[cj];
+                c.active[cj] = act;
+                c.restart[cj] = 0;
+                const double rz = c.rz[cj], nrz = c.newrz[cj];
+                c.beta[cj] = act ? nrz / (rz != 0. ? rz : 1.) : 0.;
+                c.rz[cj] = nrz;
                 act_now = act;
             }
         }
         const int nact = __syncthreads_count(act_now);
-        if (threadIdx.x == 0) {
-            c.flags[1] = check;
-            if (!check) {
-                c.flags[4] = nact;
-                if (nact == 0) c.flags[0] = 1;
+        if constexpr (SEG) {
+            if (threadIdx.x == 0) {
+                sv.segchk[x.s] = check;
+                if (!check) sv.segn[x.s] = nact;
+            }
+        }
+        if (last_segment<SEG>(tk, sv) && threadIdx.x == 0) {
+            if constexpr (!SEG) {
+                c.flags[1] = check;
+                if (!check) {
+                    c.flags[4] = nact;
+                    if (nact == 0) c.flags[0] = 1;
+                }
+            } else {
+                int any = 0;
+                for (int s = 0; s < sv.nseg; ++s) any |= __ldcg(sv.segchk + s);
+                const int total = total_active(sv);
+                c.flags[1] = any;
+                c.flags[4] = total;
+                if (!any && total == 0) c.flags[0] = 1;
             }
         }
     }
 }
 
 // ---- true residual t = q - S y; sums |t|^2 and |t - r|^2; refresh decision
-template <int MU, int SF>
-__global__ void __launch_bounds__(256) pcg_true_residual_kernel(CsrView<double> S, BsrView<double> SB,
-                                                                const double2 *q,
-                                                                const double2 *y, const double2 *r, double2 *t,
-                                                                int64_t n, RowMap mp, ColPtr c, int adaptive,
-                                                                double gap_ratio, double2 *partial, Ticket *tk,
-                                                                Counters *cnt) {
+template <int MU, int SF, bool SEG>
+__global__ void __launch_bounds__(256)
+    pcg_true_residual_kernel(CsrView<double> S, BsrView<double> SB, const double2 *q, const double2 *y,
+                             const double2 *r, double2 *t, int64_t n, RowMap mp, ColPtr c, int adaptive,
+                             double gap_ratio, double2 *partial, Ticket *tk, Counters *cnt, SegView sv) {
     if (*(volatile int *)c.flags || !*(volatile int *)(c.flags + 1)) return;
     extern __shared__ double2 smem[];
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    const Ctx x = seg_ctx<SEG>(sv, n, 0);
+    // a segment without a due check only takes part in the combine
+    const bool due = SEG ? sv.segchk[x.s] != 0 : true;
     double2 acc[MU][1];
     ZERO_ACC(acc);
-    for_rows_spmv<MU, SF>(S, SB, y, n, mp, g, lane, [&](int64_t row, const Pk<double>(&sy)[MU]) {
+    if (due) {
+        for_rows_spmv<MU, SF>(S, SB, y, x, mp, g, lane, [&](int64_t row, const Pk<double>(&sy)[MU]) {
 #pragma unroll
-        for (int m = 0; m < MU; ++m) {
-            const int u = lane + m * mp.G;
-            if (u < mp.U) {
-                const size_t o = (size_t)row * mp.U + u;
-                const double2 qv = q[o], rv = r[o];
-                const double2 tv = make_double2(qv.x - sy[m].re[0], qv.y - sy[m].im[0]);
-                t[o] = tv;
-                acc[m][0].x += tv.x * tv.x + tv.y * tv.y;
-                const double dx = tv.x - rv.x, dy = tv.y - rv.y;
-                acc[m][0].y += dx * dx + dy * dy;
+            for (int m = 0; m < MU; ++m) {
+                const int u = lane + m * mp.G;
+                if (u < mp.U) {
+                    const size_t o = (size_t)row * mp.U + u;
+                    const double2 qv = q[o], rv = r[o];
+                    const double2 tv = make_double2(qv.x - sy[m].re[0], qv.y - sy[m].im[0]);
+                    t[o] = tv;
+                    acc[m][0].x += tv.x * tv.x + tv.y * tv.y;
+                    const double dx = tv.x - rv.x, dy = tv.y - rv.y;
+                    acc[m][0].y += dx * dx + dy * dy;
+                }
             }
-        }
-    });
+        });
+    }
     cta_column_sums<MU, 1>(acc, mp, mp.U, smem, partial);
     __shared__ double2 tot[256];
-    if (tree_column_sums(partial, mp.U, tk, smem, tot)) {
+    if (seg_sums<SEG>(partial, mp.U, tk, smem, tot, sv, x)) {
         __syncthreads();
         const int j = threadIdx.x;
         bool rs = false;
-        if (j < mp.U) {
-            int act = c.active[j];
+        if (due && j < mp.U) {
+            const size_t cj = (size_t)x.s * mp.U + j;
+            int act = c.active[cj];
             int restart = 0;
             if (act) {
-                const double tn = sqrt(tot[j].x), thr = c.thr[j];
+                const double tn = sqrt(tot[j].x), thr = c.thr[cj];
                 if (adaptive) {
                     const double gap = sqrt(tot[j].y);
-                    restart = tn > thr && (gap > gap_ratio * fmax(tn, thr) || c.rn[j] <= thr);
+                    restart = tn > thr && (gap > gap_ratio * fmax(tn, thr) || c.rn[cj] <= thr);
                 } else {
                     restart = 1;
                 }
                 act = tn > thr;
-                c.tn[j] = tn;
+                c.tn[cj] = tn;
             }
-            c.active[j] = act;
-            c.restart[j] = restart;
+            c.active[cj] = act;
+            c.restart[cj] = restart;
             rs = restart;
         }
         const int nrs = __syncthreads_count(rs);
-        if (threadIdx.x == 0) {
+        if constexpr (SEG) {
+            if (threadIdx.x == 0 && nrs) atomicAdd(reinterpret_cast<unsigned long long *>(&cnt->v[2]),
+                                                   (unsigned long long)nrs);
+        }
+        if (last_segment<SEG>(tk, sv) && threadIdx.x == 0) {
             cnt->v[0] += 1;  // true_residual_refreshes
             cnt->v[1] += 1;  // true_residual_checks
-            cnt->v[2] += nrs;
+            if constexpr (!SEG) cnt->v[2] += nrs;
         }
     }
 }
 
 // ---- after a check: r <- t on restarted columns, z = M^-1 r, beta
-template <int MU, int MAXB>
-__global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB)) pcg_restart_kernel(double2 *r, double2 *z, const double2 *t, Pre P,
-                                                          int64_t nb, RowMap mp, ColPtr c, double2 *partial,
-                                                          Ticket *tk) {
+template <int MU, int MAXB, bool SEG>
+__global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
+    pcg_restart_kernel(double2 *r, double2 *z, const double2 *t, Pre P, int64_t nb, RowMap mp, ColPtr c,
+                       double2 *partial, Ticket *tk, SegView sv) {
     if (*(volatile int *)c.flags || !*(volatile int *)(c.flags + 1)) return;
     extern __shared__ double2 smem[];
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
     const int U = mp.U;
+    const Ctx x = seg_ctx<SEG>(sv, 0, nb);
+    const size_t cs0 = (size_t)x.s * U;
+    const bool due = SEG ? sv.segchk[x.s] != 0 : true;
     double2 acc[MU][1];
     ZERO_ACC(acc);
-    for (int64_t bi = (int64_t)blockIdx.x * mp.gpc + g; bi < nb; bi += (int64_t)gridDim.x * mp.gpc) {
+    for (int64_t bi = x.b0 + (int64_t)x.lc * mp.gpc + g; due && bi < x.b1; bi += (int64_t)x.nct * mp.gpc) {
         int64_t r0;
         int m;
         block_rows<MAXB>(P, bi, r0, m);
@@ -524,7 +667,7 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB)) pcg_restart_kernel(d
         for (int mm = 0; mm < MU; ++mm) {
             const int u = lane + mm * mp.G;
             if (u >= U) continue;
-            const int rs = c.restart[u];
+            const int rs = c.restart[cs0 + u];
             double2 rr[MAXB], zz[MAXB];
 #pragma unroll
             for (int i = 0; i < MAXB; ++i) {
@@ -550,56 +693,77 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB)) pcg_restart_kernel(d
     }
     cta_column_sums<MU, 1>(acc, mp, U, smem, partial);
     __shared__ double2 tot[256];
-    if (tree_column_sums(partial, U, tk, smem, tot)) {
+    if (seg_sums<SEG>(partial, U, tk, smem, tot, sv, x)) {
         __syncthreads();
         const int j = threadIdx.x;
         bool act = false;
-        if (j < U) {
-            act = c.active[j];
-            const double rz = c.rz[j], nrz = tot[j].y;
-            c.beta[j] = act ? nrz / (rz != 0. ? rz : 1.) : 0.;
-            c.rz[j] = nrz;
+        if (due && j < U) {
+            const size_t cj = cs0 + j;
+            act = c.active[cj];
+            const double rz = c.rz[cj], nrz = tot[j].y;
+            c.beta[cj] = act ? nrz / (rz != 0. ? rz : 1.) : 0.;
+            c.rz[cj] = nrz;
         }
         const int nact = __syncthreads_count(act);
-        if (threadIdx.x == 0) {
+        if constexpr (SEG) {
+            if (threadIdx.x == 0 && due) {
+                sv.segn[x.s] = nact;
+                sv.segchk[x.s] = 0;
+            }
+        }
+        if (last_segment<SEG>(tk, sv) && threadIdx.x == 0) {
+            const int total = SEG ? total_active(sv) : nact;
             c.flags[1] = 0;
-            c.flags[4] = nact;
-            if (nact == 0) c.flags[0] = 1;
+            c.flags[4] = total;
+            if (total == 0) c.flags[0] = 1;
         }
     }
 }
 
 // p = active ? z + (restart ? 0 : beta p) : 0
-__global__ void pcg_direction_kernel(const double2 *z, double2 *p, int64_t len, int U, ColPtr c) {
+__device__ __forceinline__ double2 direction(const ColPtr &c, size_t cj, double2 zv, double2 pv) {
+    if (!c.active[cj]) return make_double2(0., 0.);
+    if (c.restart[cj]) return zv;
+    const double be = c.beta[cj];
+    return make_double2(zv.x + pv.x * be, zv.y + pv.y * be);
+}
+template <bool SEG>
+__global__ void pcg_direction_kernel(const double2 *z, double2 *p, int64_t len, RowMap mp, ColPtr c, SegView sv) {
     if (*(volatile int *)c.flags) return;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int j = (int)(i % U);
-        if (!c.active[j]) {
-            p[i] = make_double2(0., 0.);
-        } else {
-            const double2 zv = z[i];
-            if (c.restart[j]) {
-                p[i] = zv;
+    if constexpr (!SEG) {
+        const int U = mp.U;
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len;
+             i += (int64_t)gridDim.x * blockDim.x) {
+            const int j = (int)(i % U);
+            if (!c.active[j]) {
+                p[i] = make_double2(0., 0.);
             } else {
-                const double2 pv = p[i];
-                const double be = c.beta[j];
-                p[i] = make_double2(zv.x + pv.x * be, zv.y + pv.y * be);
+                const double2 zv = z[i];
+                p[i] = c.restart[j] ? zv : direction(c, j, zv, p[i]);
             }
         }
+    } else {
+        const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+        const Ctx x = seg_ctx<SEG>(sv, 0, 0);
+        for (int64_t row = x.r0 + (int64_t)x.lc * mp.gpc + g; row < x.r1; row += (int64_t)x.nct * mp.gpc)
+            for (int u = lane; u < mp.U; u += mp.G) {
+                const size_t o = (size_t)row * mp.U + u;
+                p[o] = direction(c, (size_t)x.s * mp.U + u, z[o], p[o]);
+            }
     }
 }
 
 // ---- final acceptance: t = q - S y; converged, relative, residual
-template <int MU, int SF>
-__global__ void __launch_bounds__(256) pcg_final_kernel(CsrView<double> S, BsrView<double> SB, const double2 *q, const double2 *y,
-                                                        int64_t n, RowMap mp, ColPtr c, double2 *partial,
-                                                        Ticket *tk, Counters *cnt) {
+template <int MU, int SF, bool SEG>
+__global__ void __launch_bounds__(256)
+    pcg_final_kernel(CsrView<double> S, BsrView<double> SB, const double2 *q, const double2 *y, int64_t n,
+                     RowMap mp, ColPtr c, double2 *partial, Ticket *tk, Counters *cnt, SegView sv) {
     extern __shared__ double2 smem[];
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    const Ctx x = seg_ctx<SEG>(sv, n, 0);
     double2 acc[MU][1];
     ZERO_ACC(acc);
-    for_rows_spmv<MU, SF>(S, SB, y, n, mp, g, lane, [&](int64_t row, const Pk<double>(&sy)[MU]) {
+    for_rows_spmv<MU, SF>(S, SB, y, x, mp, g, lane, [&](int64_t row, const Pk<double>(&sy)[MU]) {
 #pragma unroll
         for (int m = 0; m < MU; ++m) {
             const int u = lane + m * mp.G;
@@ -612,37 +776,40 @@ __global__ void __launch_bounds__(256) pcg_final_kernel(CsrView<double> S, BsrVi
     });
     cta_column_sums<MU, 1>(acc, mp, mp.U, smem, partial);
     __shared__ double2 tot[256];
-    if (tree_column_sums(partial, mp.U, tk, smem, tot)) {
+    if (seg_sums<SEG>(partial, mp.U, tk, smem, tot, sv, x)) {
         __syncthreads();
         const int j = threadIdx.x;
         if (j < mp.U) {
-            const double rn = sqrt(tot[j].x), bn = c.bn[j];
-            c.conv[j] = rn <= c.thr[j] && !c.brk[j];
-            c.relative[j] = bn > 0. ? rn / bn : 0.;
-            c.residual[j] = rn * c.safe[j];
-            c.rn[j] = rn;
+            const size_t cj = (size_t)x.s * mp.U + j;
+            const double rn = sqrt(tot[j].x), bn = c.bn[cj];
+            c.conv[cj] = rn <= c.thr[cj] && !c.brk[cj];
+            c.relative[cj] = bn > 0. ? rn / bn : 0.;
+            c.residual[cj] = rn * c.safe[cj];
+            c.rn[cj] = rn;
         }
-        if (threadIdx.x == 0) cnt->v[1] += 1;
+        if (last_segment<SEG>(tk, sv) && threadIdx.x == 0) cnt->v[1] += 1;
     }
 }
 
 // ---- output: Y = y * safe with representability checks; status
-template <int MU>
+template <int MU, bool SEG>
 __global__ void __launch_bounds__(256) pcg_out_kernel(const double2 *y, double2 *Y, int64_t n, RowMap mp,
                                                       ColPtr c, double2 *partial, Ticket *tk, Counters *cnt,
-                                                      int *status, FailReportFull *fr) {
+                                                      int *status, FailReportFull *fr, SegView sv) {
     extern __shared__ double2 smem[];
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
+    const Ctx x = seg_ctx<SEG>(sv, n, 0);
+    const size_t cs0 = (size_t)x.s * mp.U;
     double2 acc[MU][1];
     ZERO_ACC(acc);
-    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < n; row += (int64_t)gridDim.x * mp.gpc) {
+    for (int64_t row = x.r0 + (int64_t)x.lc * mp.gpc + g; row < x.r1; row += (int64_t)x.nct * mp.gpc) {
 #pragma unroll
         for (int m = 0; m < MU; ++m) {
             const int u = lane + m * mp.G;
             if (u < mp.U) {
                 const size_t o = (size_t)row * mp.U + u;
                 const double2 v = y[o];
-                const double sf = c.safe[u];
+                const double sf = c.safe[cs0 + u];
                 const double2 w = make_double2(v.x * sf, v.y * sf);
                 Y[o] = w;
                 acc[m][0].x += (!isfinite(v.x) || !isfinite(v.y)) ? 1. : 0.;
@@ -652,48 +819,55 @@ __global__ void __launch_bounds__(256) pcg_out_kernel(const double2 *y, double2 
     }
     cta_column_sums<MU, 1>(acc, mp, mp.U, smem, partial);
     __shared__ double2 tot[256];
-    if (tree_column_sums(partial, mp.U, tk, smem, tot)) {
+    if (seg_sums<SEG>(partial, mp.U, tk, smem, tot, sv, x)) {
         __syncthreads();
         const int j = threadIdx.x;
-        bool notconv = false, unrep = false;
-        long long it = 0;
-        double rel = 0.;
         if (j < mp.U) {
+            const size_t cj = cs0 + j;
             const int fin = tot[j].x == 0. && tot[j].y == 0.;
-            c.finp[j] = tot[j].x == 0.;
-            c.fino[j] = fin;
-            c.conv[j] = c.conv[j] && fin;
-            notconv = !c.conv[j];
-            unrep = !fin;
-            it = c.iters[j];
-            rel = c.relative[j];
+            c.finp[cj] = tot[j].x == 0.;
+            c.fino[cj] = fin;
+            c.conv[cj] = c.conv[cj] && fin;
         }
-        const bool any_nc = __syncthreads_or(notconv);
-        const bool any_unrep = __syncthreads_or(unrep);
-        // max over columns of iterations and relative residual
-        __shared__ long long imax[256];
-        __shared__ double rmax[256];
-        imax[threadIdx.x] = it;
-        rmax[threadIdx.x] = rel;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            long long mi = 0;
-            double mr = cnt->max_rel;
-            for (int k = 0; k < (int)blockDim.x; ++k) {
-                mi = imax[k] > mi ? imax[k] : mi;
-                mr = fmax(mr, rmax[k]);
+        if (last_segment<SEG>(tk, sv)) {
+            // every column's state is final: reduce over all of them
+            __syncthreads();
+            const int ncols = (SEG ? sv.nseg : 1) * mp.U;
+            bool notconv = false, unrep = false;
+            long long it = 0;
+            double rel = 0.;
+            for (int k = threadIdx.x; k < ncols; k += blockDim.x) {
+                notconv |= !__ldcg(c.conv + k);
+                unrep |= !__ldcg(c.fino + k);
+                it = max(it, __ldcg(c.iters + k));
+                rel = fmax(rel, __ldcg(c.relative + k));
             }
-            cnt->v[3] += mi;
-            cnt->max_rel = mr;
-            const bool nonfinite_rhs = c.flags[2] != 0;
-            const bool brk = c.flags[3] != 0;
-            if ((any_nc || brk || nonfinite_rhs) && status != nullptr && *status == 0) {
-                *status = nonfinite_rhs ? KMSD_EINVAL : KMSD_EMETRIC;
-                status[1] = 2;  // this solve owns the failure report
-                if (fr != nullptr) {
-                    fr->head.ncols = mp.U;
-                    fr->head.code = *status;
-                    fr->head.reason = nonfinite_rhs ? 3 : any_unrep ? 2 : brk ? 1 : 0;
+            const bool any_nc = __syncthreads_or(notconv);
+            const bool any_unrep = __syncthreads_or(unrep);
+            __shared__ long long imax[256];
+            __shared__ double rmax[256];
+            imax[threadIdx.x] = it;
+            rmax[threadIdx.x] = rel;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                long long mi = 0;
+                double mr = cnt->max_rel;
+                for (int k = 0; k < (int)blockDim.x; ++k) {
+                    mi = imax[k] > mi ? imax[k] : mi;
+                    mr = fmax(mr, rmax[k]);
+                }
+                cnt->v[3] += mi;
+                cnt->max_rel = mr;
+                const bool nonfinite_rhs = c.flags[2] != 0;
+                const bool brk = c.flags[3] != 0;
+                if ((any_nc || brk || nonfinite_rhs) && status != nullptr && *status == 0) {
+                    *status = nonfinite_rhs ? KMSD_EINVAL : KMSD_EMETRIC;
+                    status[1] = 2;  // this solve owns the failure report
+                    if (fr != nullptr) {
+                        fr->head.ncols = ncols;
+                        fr->head.code = *status;
+                        fr->head.reason = nonfinite_rhs ? 3 : any_unrep ? 2 : brk ? 1 : 0;
+                    }
                 }
             }
         }
@@ -701,12 +875,12 @@ __global__ void __launch_bounds__(256) pcg_out_kernel(const double2 *y, double2 
 }
 
 // Copy the per-column report of a failed asynchronous solve (first failure).
-__global__ void pcg_copy_report_kernel(ColPtr c, int U, int *status, int *claimed, FailReportFull *fr) {
+__global__ void pcg_copy_report_kernel(ColPtr c, int ncols, int *status, int *claimed, FailReportFull *fr) {
     // Runs after pcg_out_kernel; only the solve that raised the status fills
     // the report (claimed == 2), later ones leave it unchanged.
     if (*claimed != 2) return;
     __syncthreads();
-    for (int j = threadIdx.x; j < U && j < kMaxReportCols; j += blockDim.x) {
+    for (int j = threadIdx.x; j < ncols && j < kMaxReportCols; j += blockDim.x) {
         fr->converged[j] = (uint8_t)c.conv[j];
         fr->breakdown[j] = (uint8_t)c.brk[j];
         fr->iterations[j] = c.iters[j];
@@ -720,12 +894,12 @@ __global__ void pcg_copy_report_kernel(ColPtr c, int U, int *status, int *claime
 }  // namespace
 
 // ------------------------------------------------------------------ host side
-int kmsd_metric_s::ensure(int64_t b) {
+int kmsd_metric_s::ensure(int64_t b, int64_t state_cols) {
+    if (cols.ensure(col_bytes(std::max(b, state_cols)))) return KMSD_ECUDA;
     if (b <= wb && q.p) return KMSD_OK;
     const size_t bytes = (size_t)n * b * sizeof(double2);
     for (DevBuf *d : {&q, &y, &r, &z, &p, &sp, &t})
         if (d->ensure(bytes)) return KMSD_ECUDA;
-    if (cols.ensure(col_bytes(b))) return KMSD_ECUDA;
     if (!dcount.p) {
         if (dcount.ensure(sizeof(Counters))) return KMSD_ECUDA;
         KMSD_CUDA(cudaMemset(dcount.p, 0, sizeof(Counters)));
@@ -742,57 +916,136 @@ int kmsd_metric_s::ensure(int64_t b) {
     return KMSD_OK;
 }
 
+// Device descriptor of the segments for row groups of `gpc` per CTA: CTAs
+// are shared out in proportion to each segment's rows (at least one each,
+// about one wave in total); tickets and level-2 partial rows per segment.
+int kmsd_metric_s::seg_plan(int gpc, SegPlan **out) {
+    auto it = seg_plans.find(gpc);
+    if (it != seg_plans.end()) {
+        *out = &it->second;
+        return KMSD_OK;
+    }
+    const int64_t ns = nseg;
+    std::vector<int64_t> want(ns);
+    int64_t total = 0;
+    for (int64_t s = 0; s < ns; ++s) {
+        const int64_t rows = seg_row0[s + 1] - seg_row0[s];
+        want[s] = std::max<int64_t>(1, (rows + 4 * gpc - 1) / (4 * gpc));
+        total += want[s];
+    }
+    const int64_t cap = (int64_t)sm_count() * 8;
+    std::vector<int> cta0(ns + 1, 0), tk0(ns + 1, 0), l2(ns, 0), cta_seg;
+    int l2rows = 0;
+    for (int64_t s = 0; s < ns; ++s) {
+        const int64_t k = total > cap ? std::max<int64_t>(1, want[s] * cap / total) : want[s];
+        cta0[s + 1] = cta0[s] + (int)k;
+        tk0[s + 1] = tk0[s] + range_tickets((int)k);
+        l2[s] = l2rows;
+        const int groups = ((int)k + kTreeFan - 1) / kTreeFan;
+        if (groups > 1) l2rows += groups;
+        for (int64_t q = 0; q < k; ++q) cta_seg.push_back((int)s);
+    }
+    const int grid = cta0[ns];
+    const int ntk = tk0[ns] + 1;  // plus the last-segment ticket
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t o_row = 0, o_blk = o_row + al((ns + 1) * 8), o_cseg = o_blk + al((ns + 1) * 8);
+    const size_t o_cta0 = o_cseg + al((size_t)grid * 4), o_tk0 = o_cta0 + al((ns + 1) * 4);
+    const size_t o_l2 = o_tk0 + al((ns + 1) * 4), o_segn = o_l2 + al(ns * 4), o_chk = o_segn + al(ns * 4);
+    const size_t o_tick = o_chk + al(ns * 4), bytes = o_tick + al((size_t)ntk * sizeof(Ticket));
+    SegPlan pl;
+    if (pl.mem.ensure(bytes)) return KMSD_ECUDA;
+    char *base = pl.mem.as<char>();
+    KMSD_CUDA(cudaMemset(base, 0, bytes));
+    KMSD_CUDA(cudaMemcpy(base + o_row, seg_row0.data(), (ns + 1) * 8, cudaMemcpyHostToDevice));
+    KMSD_CUDA(cudaMemcpy(base + o_blk, seg_blk0.data(), (ns + 1) * 8, cudaMemcpyHostToDevice));
+    KMSD_CUDA(cudaMemcpy(base + o_cseg, cta_seg.data(), (size_t)grid * 4, cudaMemcpyHostToDevice));
+    KMSD_CUDA(cudaMemcpy(base + o_cta0, cta0.data(), (ns + 1) * 4, cudaMemcpyHostToDevice));
+    KMSD_CUDA(cudaMemcpy(base + o_tk0, tk0.data(), (ns + 1) * 4, cudaMemcpyHostToDevice));
+    KMSD_CUDA(cudaMemcpy(base + o_l2, l2.data(), ns * 4, cudaMemcpyHostToDevice));
+    pl.row0 = reinterpret_cast<int64_t *>(base + o_row);
+    pl.blk0 = reinterpret_cast<int64_t *>(base + o_blk);
+    pl.cta_seg = reinterpret_cast<int *>(base + o_cseg);
+    pl.cta0 = reinterpret_cast<int *>(base + o_cta0);
+    pl.tk0 = reinterpret_cast<int *>(base + o_tk0);
+    pl.l2 = reinterpret_cast<int *>(base + o_l2);
+    pl.segn = reinterpret_cast<int *>(base + o_segn);
+    pl.segchk = reinterpret_cast<int *>(base + o_chk);
+    pl.tickets = reinterpret_cast<Ticket *>(base + o_tick);
+    pl.grid = grid;
+    pl.l2rows = l2rows;
+    auto ins = seg_plans.emplace(gpc, pl);
+    pl.mem.p = nullptr;  // owned by the map entry now
+    *out = &ins.first->second;
+    return KMSD_OK;
+}
+
 namespace {
 
-template <int MU, int MAXB, int SF>
+template <int MU, int MAXB, int SF, bool SEG>
 int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rtol, double atol, int maxiter,
             cudaStream_t s, int *status, FailReportFull *fr, int *claimed) {
     const int64_t n = M->n;
     const RowMap mp = make_map((int)b, kThreads);
     const int64_t nb = MAXB == 1 ? n : M->nblocks;
-    const int grid_r = grid_for(n, mp), grid_b = grid_for(nb, mp);
-    // S products walk block rows when S is stored as 4x4 blocks
-    const int grid_s = SF != S_CSR ? grid_for(M->S->bsr_nb, mp) : grid_r;
     const BsrView<double> SB = M->S->bsr64();
-    const int grid_mx = grid_r > grid_b ? grid_r : grid_b;
-    if (M->red.ensure(grid_mx, (int)b)) return KMSD_ECUDA;
     const size_t sm = reduce_smem(mp, 1);
-    ColPtr c = col_ptr(M->cols.p, b);
+    const int64_t len = n * b;
+    int grid_r, grid_b, grid_s, egrid;
+    SegView sv{};
+    sv.nseg = 1;
+    Ticket *tk;
+    if constexpr (SEG) {
+        // one grid for every kernel: each CTA belongs to one segment
+        kmsd_metric_s::SegPlan *pl = nullptr;
+        if (int rc = M->seg_plan(mp.gpc, &pl)) return rc;
+        grid_r = grid_b = grid_s = egrid = pl->grid;
+        if (M->red.ensure(pl->grid + pl->l2rows, (int)b)) return KMSD_ECUDA;
+        sv = SegView{(int)M->nseg, pl->cta_seg, pl->cta0, pl->row0, pl->blk0, pl->tk0, pl->l2, pl->segn, pl->segchk};
+        tk = pl->tickets;
+    } else {
+        grid_r = grid_for(n, mp);
+        grid_b = grid_for(nb, mp);
+        // S products walk block rows when S is stored as 4x4 blocks
+        grid_s = SF != S_CSR ? grid_for(M->S->bsr_nb, mp) : grid_r;
+        egrid = (int)std::min<int64_t>((len + 255) / 256, (int64_t)sm_count() * 16);
+        if (M->red.ensure(std::max(grid_r, std::max(grid_b, grid_s)), (int)b)) return KMSD_ECUDA;
+        tk = M->red.tick();
+    }
+    const int64_t ncols = (int64_t)sv.nseg * b;
+    ColPtr c = col_ptr(M->cols.p, ncols);
     Pre P{M->diag, M->bstart, M->foff, M->factors, M->ub};
     const CsrView<double> S = M->S->view64();
     Counters *cnt = M->dcount.as<Counters>();
     double2 *q = M->q.as<double2>(), *y = M->y.as<double2>(), *r = M->r.as<double2>(), *z = M->z.as<double2>(),
             *p = M->p.as<double2>(), *sp = M->sp.as<double2>(), *t = M->t.as<double2>();
     double2 *part = M->red.part();
-    Ticket *tk = M->red.tick();
-    const int64_t len = n * b;
-    const int egrid = (int)std::min<int64_t>((len + 255) / 256, (int64_t)sm_count() * 16);
 
     KMSD_CUDA(cudaMemsetAsync(c.flags, 0, 8 * sizeof(int), s));
-    pcg_scale_kernel<MU><<<grid_r, kThreads, sm, s>>>(B, n, mp, c, reinterpret_cast<double *>(part), tk);
+    pcg_scale_kernel<MU, SEG><<<grid_r, kThreads, sm, s>>>(B, n, mp, c, reinterpret_cast<double *>(part), tk, sv);
     count_launch();
-    pcg_init_kernel<MU, MAXB><<<grid_b, kThreads, sm, s>>>(B, q, y, r, z, P, nb, mp, c, rtol, atol, part, tk);
+    pcg_init_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, s>>>(B, q, y, r, z, P, nb, mp, c, rtol, atol, part, tk,
+                                                                sv);
     count_launch();
-    pcg_pinit_kernel<<<egrid, 256, 0, s>>>(z, p, len, (int)b, c);
+    pcg_pinit_kernel<SEG><<<egrid, 256, 0, s>>>(z, p, len, mp, c, sv);
     count_launch();
     volatile int *hflag = static_cast<volatile int *>(M->host_pinned.p);
     const int chunk = 4;
     int slot = 0, pending = 0;
     for (int k = 0; k < maxiter; ++k) {
         const int refresh = ((k + 1) % M->interval) == 0;
-        pcg_spmv_kernel<MU, SF><<<grid_s, kThreads, sm, s>>>(S, SB, p, sp, n, mp, c, part, tk);
+        pcg_spmv_kernel<MU, SF, SEG><<<grid_s, kThreads, sm, s>>>(S, SB, p, sp, n, mp, c, part, tk, sv);
         count_launch();
-        pcg_update_kernel<MU, MAXB><<<grid_b, kThreads, sm, s>>>(y, r, z, p, sp, P, nb, mp, c, refresh,
-                                                                 M->adaptive, part, tk);
+        pcg_update_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, s>>>(y, r, z, p, sp, P, nb, mp, c, refresh,
+                                                                      M->adaptive, part, tk, sv);
         count_launch();
         if (refresh || M->adaptive) {
-            pcg_true_residual_kernel<MU, SF><<<grid_s, kThreads, sm, s>>>(S, SB, q, y, r, t, n, mp, c,
-                                                                         M->adaptive, M->gap_ratio, part, tk, cnt);
+            pcg_true_residual_kernel<MU, SF, SEG><<<grid_s, kThreads, sm, s>>>(
+                S, SB, q, y, r, t, n, mp, c, M->adaptive, M->gap_ratio, part, tk, cnt, sv);
             count_launch();
-            pcg_restart_kernel<MU, MAXB><<<grid_b, kThreads, sm, s>>>(r, z, t, P, nb, mp, c, part, tk);
+            pcg_restart_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, s>>>(r, z, t, P, nb, mp, c, part, tk, sv);
             count_launch();
         }
-        pcg_direction_kernel<<<egrid, 256, 0, s>>>(z, p, len, (int)b, c);
+        pcg_direction_kernel<SEG><<<egrid, 256, 0, s>>>(z, p, len, mp, c, sv);
         count_launch();
         if ((k + 1) % chunk == 0) {
             KMSD_CUDA(cudaMemcpyAsync((void *)(hflag + slot), c.flags, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -807,12 +1060,12 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
         }
     }
     KMSD_CUDA(cudaGetLastError());
-    pcg_final_kernel<MU, SF><<<grid_s, kThreads, sm, s>>>(S, SB, q, y, n, mp, c, part, tk, cnt);
+    pcg_final_kernel<MU, SF, SEG><<<grid_s, kThreads, sm, s>>>(S, SB, q, y, n, mp, c, part, tk, cnt, sv);
     count_launch();
-    pcg_out_kernel<MU><<<grid_r, kThreads, sm, s>>>(y, Y, n, mp, c, part, tk, cnt, status, fr);
+    pcg_out_kernel<MU, SEG><<<grid_r, kThreads, sm, s>>>(y, Y, n, mp, c, part, tk, cnt, status, fr, sv);
     count_launch();
     if (status != nullptr && fr != nullptr) {
-        pcg_copy_report_kernel<<<1, 256, 0, s>>>(c, (int)b, status, claimed, fr);
+        pcg_copy_report_kernel<<<1, 256, 0, s>>>(c, (int)ncols, status, claimed, fr);
         count_launch();
     }
     KMSD_CUDA(cudaGetLastError());
@@ -822,29 +1075,31 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
 using PcgFn = int (*)(kmsd_metric_s *, const double2 *, double2 *, int64_t, double, double, int, cudaStream_t,
                       int *, FailReportFull *, int *);
 
-template <int MAXB, int SF>
+template <int MAXB, int SF, bool SEG>
 PcgFn pick_mu(int mu) {
     switch (mu) {
-        case 1: return run_pcg<1, MAXB, SF>;
-        case 2: return run_pcg<2, MAXB, SF>;
+        case 1: return run_pcg<1, MAXB, SF, SEG>;
+        case 2: return run_pcg<2, MAXB, SF, SEG>;
     }
     return nullptr;
 }
-template <int SF>
+template <int SF, bool SEG>
 PcgFn pick_b(int mu, int maxb) {
-    if (maxb <= 1) return pick_mu<1, SF>(mu);
-    if (maxb <= 4) return pick_mu<4, SF>(mu);
-    if (maxb <= 8) return pick_mu<8, SF>(mu);
-    if (maxb <= 32) return pick_mu<32, SF>(mu);
+    if (maxb <= 1) return pick_mu<1, SF, SEG>(mu);
+    if (maxb <= 4) return pick_mu<4, SF, SEG>(mu);
+    if (maxb <= 8) return pick_mu<8, SF, SEG>(mu);
+    if (maxb <= 32) return pick_mu<32, SF, SEG>(mu);
     return nullptr;
 }
-PcgFn pick(int mu, int maxb, int sf) {
+template <bool SEG>
+PcgFn pick_s(int mu, int maxb, int sf) {
     switch (sf) {
-        case S_BSR_REAL: return pick_b<S_BSR_REAL>(mu, maxb);
-        case S_BSR_CPLX: return pick_b<S_BSR_CPLX>(mu, maxb);
+        case S_BSR_REAL: return pick_b<S_BSR_REAL, SEG>(mu, maxb);
+        case S_BSR_CPLX: return pick_b<S_BSR_CPLX, SEG>(mu, maxb);
     }
-    return pick_b<S_CSR>(mu, maxb);
+    return pick_b<S_CSR, SEG>(mu, maxb);
 }
+PcgFn pick(int mu, int maxb, int sf, bool seg) { return seg ? pick_s<true>(mu, maxb, sf) : pick_s<false>(mu, maxb, sf); }
 
 }  // namespace
 
@@ -854,10 +1109,14 @@ int kmsd_metric_s::solve(const double2 *B, double2 *Y, int64_t b, double rtol, d
         return fail(KMSD_EINVAL, "invalid metric RHS shape/tolerances");
     if (b > 256) return fail(KMSD_EINVAL, "metric solve supports at most 256 columns per call");
     const auto start = std::chrono::steady_clock::now();
-    if (ensure(b)) return KMSD_ECUDA;
+    const bool seg = nseg > 1;
+    const int64_t ncols = seg ? nseg * b : b;
+    if (ensure(b, ncols)) return KMSD_ECUDA;
     const RowMap mp = make_map((int)b, kThreads);
-    const int sf = S->bsr_nb > 0 ? (S->bsr64().im ? S_BSR_CPLX : S_BSR_REAL) : S_CSR;
-    PcgFn fn = pick(mu_for(mp), nblocks ? maxb : 1, sf);
+    // 4x4 block rows may not straddle two segments
+    const bool bsr = S->bsr_nb > 0 && (!seg || seg_aligned4);
+    const int sf = bsr ? (S->bsr64().im ? S_BSR_CPLX : S_BSR_REAL) : S_CSR;
+    PcgFn fn = pick(mu_for(mp), nblocks ? maxb : 1, sf, seg);
     if (!fn) return fail(KMSD_EINVAL, "unsupported metric block size / column count");
     const bool sync = status == nullptr;
     // Synchronous calls use a private status word and report.
@@ -877,23 +1136,23 @@ int kmsd_metric_s::solve(const double2 *B, double2 *Y, int64_t b, double rtol, d
     if (rc) return rc;
     ++calls;
     if (!sync) return KMSD_OK;
-    // Read status + per-column report.
-    ColPtr c = col_ptr(cols.p, b);
-    std::vector<int> conv(b), brk(b), flags(8);
-    std::vector<long long> it(b);
-    std::vector<double> res(b), rel(b);
+    // Read status + per-column report (segment-major for a segmented solve).
+    ColPtr c = col_ptr(cols.p, ncols);
+    std::vector<int> conv(ncols), brk(ncols), flags(8);
+    std::vector<long long> it(ncols);
+    std::vector<double> res(ncols), rel(ncols);
     int hst[2];
-    KMSD_CUDA(cudaMemcpyAsync(conv.data(), c.conv, b * sizeof(int), cudaMemcpyDeviceToHost, s));
-    KMSD_CUDA(cudaMemcpyAsync(brk.data(), c.brk, b * sizeof(int), cudaMemcpyDeviceToHost, s));
-    KMSD_CUDA(cudaMemcpyAsync(it.data(), c.iters, b * sizeof(long long), cudaMemcpyDeviceToHost, s));
-    KMSD_CUDA(cudaMemcpyAsync(res.data(), c.residual, b * sizeof(double), cudaMemcpyDeviceToHost, s));
-    KMSD_CUDA(cudaMemcpyAsync(rel.data(), c.relative, b * sizeof(double), cudaMemcpyDeviceToHost, s));
+    KMSD_CUDA(cudaMemcpyAsync(conv.data(), c.conv, ncols * sizeof(int), cudaMemcpyDeviceToHost, s));
+    KMSD_CUDA(cudaMemcpyAsync(brk.data(), c.brk, ncols * sizeof(int), cudaMemcpyDeviceToHost, s));
+    KMSD_CUDA(cudaMemcpyAsync(it.data(), c.iters, ncols * sizeof(long long), cudaMemcpyDeviceToHost, s));
+    KMSD_CUDA(cudaMemcpyAsync(res.data(), c.residual, ncols * sizeof(double), cudaMemcpyDeviceToHost, s));
+    KMSD_CUDA(cudaMemcpyAsync(rel.data(), c.relative, ncols * sizeof(double), cudaMemcpyDeviceToHost, s));
     KMSD_CUDA(cudaMemcpyAsync(flags.data(), c.flags, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
     KMSD_CUDA(cudaMemcpyAsync(hst, st, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     KMSD_CUDA(cudaStreamSynchronize(s));
     seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
     if (report) {
-        for (int64_t j = 0; j < b; ++j) {
+        for (int64_t j = 0; j < ncols; ++j) {
             report->converged[j] = (uint8_t)conv[j];
             report->breakdown[j] = (uint8_t)brk[j];
             report->iterations[j] = it[j];
@@ -904,10 +1163,10 @@ int kmsd_metric_s::solve(const double2 *B, double2 *Y, int64_t b, double rtol, d
     if (flags[2]) return fail(KMSD_EINVAL, "metric RHS must be finite");
     if (hst[0]) {
         // Reproduce the reference's message precedence (native.cpp:447-450).
-        std::vector<int> finp(b), fino(b);
-        KMSD_CUDA(cudaMemcpy(fino.data(), c.fino, b * sizeof(int), cudaMemcpyDeviceToHost));
+        std::vector<int> fino(ncols);
+        KMSD_CUDA(cudaMemcpy(fino.data(), c.fino, ncols * sizeof(int), cudaMemcpyDeviceToHost));
         bool representable = true;
-        for (int64_t j = 0; j < b; ++j) representable = representable && fino[j];
+        for (int64_t j = 0; j < ncols; ++j) representable = representable && fino[j];
         if (!representable)
             return fail(KMSD_EMETRIC,
                         "S solve solution is nonfinite or not representable in complex128 after rescaling");
@@ -1002,6 +1261,7 @@ int kmsd_metric_create(kmsd_csr s, const double *diag, int64_t nblocks, const in
     M->n = n;
     M->nblocks = nblocks;
     M->maxb = maxb;
+    M->bstart_host.assign(bs.begin(), bs.end());
     // Uniform partition with factors packed in block order (atom blocks of
     // one size): the kernels then compute rows and factor offsets directly.
     if (nblocks > 0) {
@@ -1047,9 +1307,74 @@ void kmsd_metric_destroy(kmsd_metric m) {
     m->red.partial.release();
     m->red.ticket.release();
     if (m->host_pinned.p) cudaFreeHost(m->host_pinned.p);
+    for (auto &kv : m->seg_plans) kv.second.mem.release();
     for (auto &e : m->ev)
         if (e) cudaEventDestroy(e);
     delete m;
+}
+
+namespace {
+// bad[0] = 1 when a row of S has an entry outside its segment's rows.
+__global__ void seg_coupling_kernel(const int *ptr, const int *idx, int64_t n, const int64_t *row0, int nseg,
+                                    int *bad) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nseg - 1;  // segment of row r: row0[lo] <= r < row0[lo + 1]
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (row0[mid] <= r) lo = mid;
+            else hi = mid - 1;
+        }
+        const int64_t a = row0[lo], b = row0[lo + 1];
+        for (int k = ptr[r]; k < ptr[r + 1]; ++k)
+            if (idx[k] < a || idx[k] >= b) bad[0] = 1;
+    }
+}
+}  // namespace
+
+int kmsd_metric_set_segments(kmsd_metric m, int64_t nseg, const int64_t *row_offsets) {
+    if (!m) return fail(KMSD_EINVAL, "invalid metric segments");
+    for (auto &kv : m->seg_plans) kv.second.mem.release();
+    m->seg_plans.clear();
+    m->nseg = 0;
+    m->seg_row0.clear();
+    m->seg_blk0.clear();
+    if (nseg <= 1) return KMSD_OK;
+    if (!row_offsets || row_offsets[0] != 0 || row_offsets[nseg] != m->n)
+        return fail(KMSD_EINVAL, "segment offsets must run from 0 to the metric size");
+    for (int64_t s = 0; s < nseg; ++s)
+        if (row_offsets[s + 1] <= row_offsets[s]) return fail(KMSD_EINVAL, "segment offsets must increase");
+    std::vector<int64_t> blk(nseg + 1);
+    if (m->nblocks > 0) {
+        int64_t k = 0;
+        for (int64_t s = 0; s <= nseg; ++s) {
+            while (k < m->nblocks && m->bstart_host[k] < row_offsets[s]) ++k;
+            if (m->bstart_host[k] != row_offsets[s])
+                return fail(KMSD_EINVAL, "block-Jacobi blocks cross a segment boundary");
+            blk[s] = k;
+        }
+    } else {
+        blk.assign(row_offsets, row_offsets + nseg + 1);
+    }
+    // S must be block-diagonal over the segments
+    DevBuf chk;
+    if (chk.ensure((size_t)(nseg + 1) * 8 + 256)) return KMSD_ECUDA;
+    int64_t *d_row0 = chk.as<int64_t>();
+    int *d_bad = reinterpret_cast<int *>(reinterpret_cast<char *>(chk.p) + (size_t)(nseg + 1) * 8 + 128);
+    int bad = 0;
+    KMSD_CUDA(cudaMemcpy(d_row0, row_offsets, (size_t)(nseg + 1) * 8, cudaMemcpyHostToDevice));
+    KMSD_CUDA(cudaMemset(d_bad, 0, sizeof(int)));
+    const int grid = (int)std::min<int64_t>((m->n + 255) / 256, (int64_t)sm_count() * 8);
+    seg_coupling_kernel<<<grid, 256>>>(m->S->ptr, m->S->idx, m->n, d_row0, (int)nseg, d_bad);
+    count_launch();
+    KMSD_CUDA(cudaMemcpy(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost));
+    chk.release();
+    if (bad) return fail(KMSD_EINVAL, "S couples two segments; a segmented solve needs a block-diagonal S");
+    m->nseg = nseg;
+    m->seg_row0.assign(row_offsets, row_offsets + nseg + 1);
+    m->seg_blk0 = blk;
+    m->seg_aligned4 = true;
+    for (int64_t s = 0; s <= nseg; ++s) m->seg_aligned4 = m->seg_aligned4 && row_offsets[s] % 4 == 0;
+    return KMSD_OK;
 }
 
 int kmsd_metric_set_residual_policy(kmsd_metric m, int policy, int interval, double gap_ratio) {

@@ -233,6 +233,7 @@ class B200Metric:
                        getattr(config, "metric_gap_ratio", .1))
         self._set_policy(*self.policy)
         self.identity = bool(self.lib.kmsd_metric_is_identity(handle))
+        self.nseg = 1
 
     def replica(self):
         """A second metric over the same uploaded S with its own workspace, for
@@ -273,6 +274,17 @@ class B200Metric:
                        getattr(config, "metric_gap_ratio", .1))
         self._set_policy(*self.policy)
         self.identity = bool(self.lib.kmsd_metric_is_identity(handle))
+        self.nseg = 1
+
+    def set_segments(self, offsets):
+        """Declare S block-diagonal over the row ranges offsets[s]:offsets[s+1]
+        (independent systems); later solves run one CG per (segment, column)
+        and report nseg * b entries, segment-major (kmsd_metric_set_segments)."""
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        nseg = len(off) - 1
+        _check(self.lib, self.lib.kmsd_metric_set_segments(self.handle, nseg,
+                                                          off.ctypes.data_as(C.POINTER(C.c_int64))))
+        self.nseg = max(nseg, 1)
 
     def _set_policy(self, policy, interval, gap):
         _check(self.lib, self.lib.kmsd_metric_set_residual_policy(
@@ -283,12 +295,15 @@ class B200Metric:
         t, host = as_device(B, self.n)
         out = torch.empty_like(t)
         b = t.shape[1]
+        nseg = getattr(self, "nseg", 1)
+        if nseg > 1 and b > MAX_COLS:
+            raise ValueError(f"a segmented solve takes at most {MAX_COLS} columns per call")
         reps = []
         for j0 in range(0, b, MAX_COLS):
             j1 = min(b, j0 + MAX_COLS)
             x = t[:, j0:j1].contiguous()
             y = torch.empty_like(x)
-            rep, arrays = _report_arrays(j1 - j0)
+            rep, arrays = _report_arrays(nseg * (j1 - j0))
             rc = self.lib.kmsd_metric_solve(self.handle, _ptr(x), _ptr(y), j1 - j0, float(rtol), float(atol),
                                             int(maxiter), C.byref(rep), _stream(torch))
             if rc == _abi.KMSD_EMETRIC:
