@@ -57,9 +57,10 @@ def parse():
     p.add_argument("--moments", type=int, default=4096)
     p.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     p.add_argument("--method", choices=["doubling", "direct"], default="doubling")
-    p.add_argument("--workload", choices=["honeycomb", "diamond", "serving"], default="honeycomb",
+    p.add_argument("--workload", choices=["honeycomb", "diamond", "batch", "serving"], default="honeycomb",
                    help="honeycomb: the headline KPM-moment workload; diamond: the nonorthogonal sp3 model "
                         "(8000 atoms x 4 orbitals, kappa(S)=50, block-Jacobi PCG to 1e-10, R=32, M=1024); "
+                        "batch: a ragged batch of 32 nonorthogonal sp3 instances (4,000-32,000 orbitals), R=16; "
                         "serving: a Poisson request stream through the continuous-batching service")
     p.add_argument("--no-compare", action="store_true", help="skip the FP64 / direct comparison lines")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -228,6 +229,86 @@ def run_diamond(args):
                       "mu0_over_n": float(mu[0].mean().item()) / m.n}))
 
 
+def run_batch(args):
+    """Ragged batch of nonorthogonal instances (a sample of the 256-instance,
+    4k-400k-orbital batching config): 32 diamond sp3 instances with
+    log-uniform cell counts 5..10 (4,000-32,000 orbitals), disorder
+    W_i ~ U[0.1, 2] eV, kappa(S)=50, block-Jacobi PCG to 1e-10, FP64, R=16,
+    M=64 by default.  One batch call (one segmented PCG over all instances per
+    step) is timed against separate per-instance engine calls."""
+    import scipy.linalg as la
+    import scipy.sparse as sp
+    import torch
+    from types import SimpleNamespace
+    from kubomsd_b200 import _abi, kpm, lattices
+    from kubomsd_b200.batch import B200Batch
+    from kubomsd_b200.native import B200Metric, B200Operators
+    lib = _abi.require_library()
+    rng = np.random.default_rng(4)
+    cells = np.round(np.exp(rng.uniform(np.log(5), np.log(10), 32))).astype(int)
+    W = rng.uniform(.1, 2., 32)
+    ms = [lattices.diamond_sp3(cells=int(c), W=float(w), seed=100 + i) for i, (c, w) in enumerate(zip(cells, W))]
+    Hs, Ss = [m.H for m in ms], [sp.csr_matrix(m.S) for m in ms]
+    blocks = [[(a, b, la.cholesky(S[a:b, a:b].toarray(), lower=True)) for a, b in m.atom_slices]
+              for m, S in zip(ms, Ss)]
+    R, M = 16, args.moments if args.moments != 4096 else 64
+    c, a = 0., 40.
+    phases = [torch.from_numpy(kpm.random_phases(m.n, 20261019 + i, range(R))).cuda() for i, m in enumerate(ms)]
+    bt = B200Batch(Hs, precision="fp64", overlaps=Ss, blocks=blocks, rtol=1e-10)
+    B = bt.concat(phases)
+    N = bt.n
+    for _ in range(args.warmup):
+        bt.moments(B, min(M, 16), c, a)
+    st0 = bt.metric.stats()
+    torch.cuda.synchronize()
+    l0 = lib.kmsd_kernel_launches()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(args.steps):
+        mu = bt.moments(B, M, c, a)
+    e.record()
+    torch.cuda.synchronize()
+    ms_batch = s.elapsed_time(e) / args.steps
+    st1 = bt.metric.stats()
+    launches = int(lib.kmsd_kernel_launches() - l0)
+    solves = (st1.calls - st0.calls) / args.steps
+    iters = (st1.max_iterations_sum - st0.max_iterations_sum) / max(st1.calls - st0.calls, 1)
+    # the same instances through separate engine calls, one after another
+    cfg = SimpleNamespace(metric_rtol=1e-10, metric_atol=0., metric_maxiter=1000, metric_residual_policy="fixed",
+                          metric_check_interval=32, metric_gap_ratio=.1, metric_solver="pcg", precision="fp64",
+                          moment_doubling=False)
+    engines = []
+    for H, S, bl in zip(Hs, Ss, blocks):
+        met = B200Metric(S, S.diagonal().real.copy(), bl, cfg)
+        engines.append(B200Operators(SimpleNamespace(host_H=H, metric=SimpleNamespace(native=met), velocity={},
+                                                     position={}, composite={}), cfg))
+    for eng, ph in zip(engines, phases):
+        eng.moments(ph, 2, c, a)
+    torch.cuda.synchronize()
+    s.record()
+    sep = [eng.moments(ph, M, c, a) for eng, ph in zip(engines, phases)]
+    e.record()
+    torch.cuda.synchronize()
+    ms_sep = s.elapsed_time(e)
+    host = lambda x: x.cpu().numpy() if hasattr(x, "cpu") else np.asarray(x)  # noqa: E731
+    err = max(float(np.max(np.abs(host(mu[i]) - host(sep[i]))) / float(np.max(np.abs(host(sep[i])))))
+              for i in range(len(ms)))
+    print(json.dumps({"metric": METRIC, "value": N * M * R / (ms_batch / 1e3), "unit": UNIT, "n_gpus": 1,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batch, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+                      "data": "synthetic (seeded diamond sp3 instances, NumPy PCG64 phases)",
+                      "config": {"workload": f"ragged batch of {len(ms)} nonorthogonal diamond sp3 instances, "
+                                             f"{int(min(m.n for m in ms)):,}-{int(max(m.n for m in ms)):,} orbitals "
+                                             f"({N:,} in total), kappa(S)=50, block-Jacobi PCG rtol 1e-10, R={R}, "
+                                             f"M={M}, FP64",
+                                 "spectral_bounds_eV": [c - a, c + a], "segmented_solves_per_step": solves,
+                                 "pcg_iterations_per_solve": iters},
+                      "gpu_launches": launches,
+                      "separate_calls": {"ms": ms_sep, "value": N * M * R / (ms_sep / 1e3),
+                                         "speedup_of_batch": ms_sep / ms_batch,
+                                         "max_rel_diff_vs_batch": err}}))
+
+
 def run_serving(args):
     """Config 5 (shortened): Poisson stream of KPM DOS jobs over resident
     orthogonal 2D lattices and nonorthogonal sp3 cells, admitted by an HBM
@@ -274,6 +355,9 @@ def main():
         return
     if args.workload == "serving":
         run_serving(args)
+        return
+    if args.workload == "batch":
+        run_batch(args)
         return
     import torch
     import torch.distributed as dist
