@@ -219,6 +219,7 @@ struct kmsd_batch_s {
     double rtol = 1e-10, atol = 0.;
     int maxiter = 1000;
     DevBuf hx, t1, status, report;
+    int64_t general_kernels = 0;  // host-side kernels recorded in the nonorthogonal graph
 };
 
 namespace {
@@ -356,16 +357,22 @@ void launch_tiles(const BatchArgs<T> &a, int64_t ntiles, cudaStream_t s) {
 // segmented PCG over every instance's S (one CG per instance and column),
 // and one tile step kernel on the solved operand; mu_k = Re<S B, T_k> per
 // instance (Engine::moments, cpp/native.cpp:590-609, for each instance).
-template <int MU>
-int run_general(kmsd_batch_s *bt, const double2 *B, double *mu, int64_t b, int64_t length, cudaStream_t s) {
-    const int64_t n = bt->n;
-    const RowMap mp = make_map((int)b, kThreads);
-    const int ncol = (int)b;
-    const size_t vb = (size_t)n * b * sizeof(double2);
+// Everything the nonorthogonal sequence allocates, done before any capture.
+int prepare_general(kmsd_batch_s *bt, const double2 *B, int64_t b, cudaStream_t s) {
+    const size_t vb = (size_t)bt->n * b * sizeof(double2);
     if (bt->ta.ensure(vb) || bt->tb.ensure(vb) || bt->bra.ensure(vb) || bt->hx.ensure(vb) || bt->t1.ensure(vb) ||
-        bt->partial.ensure((size_t)bt->tiles.ntiles * ncol * 2 * sizeof(double2) + 256) ||
+        bt->partial.ensure((size_t)bt->tiles.ntiles * b * 2 * sizeof(double2) + 256) ||
         bt->status.ensure(4 * sizeof(int)) || bt->report.ensure(sizeof(FailReportFull)))
         return KMSD_ECUDA;
+    return bt->gm->prepare_dev(b);
+}
+
+// The launches of a nonorthogonal moments call (recorded into a graph, or
+// run as they are); the status word is read by the caller.
+template <int MU>
+int record_general(kmsd_batch_s *bt, const double2 *B, double *mu, int64_t b, int64_t length, cudaStream_t s) {
+    const RowMap mp = make_map((int)b, kThreads);
+    const int ncol = (int)b;
     int *status = bt->status.as<int>();
     KMSD_CUDA(cudaMemsetAsync(status, 0, 4 * sizeof(int), s));
     double2 *ta = bt->ta.as<double2>(), *tb = bt->tb.as<double2>(), *sb = bt->bra.as<double2>();
@@ -396,7 +403,7 @@ int run_general(kmsd_batch_s *bt, const double2 *B, double *mu, int64_t b, int64
     for (int64_t k = 1; k < length; ++k) {
         double2 *next = k == 1 ? ta : k == 2 ? tb : const_cast<double2 *>(prev);
         if ((rc = spmm64(bt->gh, curr, t1, b, s))) return rc;
-        if ((rc = bt->gm->solve(t1, hx, b, bt->rtol, bt->atol, bt->maxiter, nullptr, s, status, bt->report.p)))
+        if ((rc = bt->gm->solve_dev(t1, hx, b, bt->rtol, bt->atol, bt->maxiter, s, status, bt->report.p)))
             return rc;
         a.curr = curr;
         a.prev = prev;
@@ -410,9 +417,13 @@ int run_general(kmsd_batch_s *bt, const double2 *B, double *mu, int64_t b, int64
         curr = next;
     }
     KMSD_CUDA(cudaGetLastError());
-    // a failed solve of any instance fails the call with the reference's message
+    return KMSD_OK;
+}
+
+// A failed solve of any instance fails the call with the reference's message.
+int general_status(kmsd_batch_s *bt, cudaStream_t s) {
     int st[4];
-    KMSD_CUDA(cudaMemcpyAsync(st, status, sizeof(st), cudaMemcpyDeviceToHost, s));
+    KMSD_CUDA(cudaMemcpyAsync(st, bt->status.as<int>(), sizeof(st), cudaMemcpyDeviceToHost, s));
     KMSD_CUDA(cudaStreamSynchronize(s));
     if (st[0] != 0) {
         FailReportFull fr;
@@ -524,8 +535,56 @@ int batch_call(kmsd_batch_s *bt, const void *b_in, double *mu, int64_t b, int64_
         const RowMap mp = make_map((int)b, kThreads);
         const int m = mu_for(mp);
         if (!m || b > 256) return fail(KMSD_EINVAL, "too many columns for one batch call");
-        return m == 1 ? run_general<1>(bt, static_cast<const double2 *>(b_in), mu, b, length, s)
-                      : run_general<2>(bt, static_cast<const double2 *>(b_in), mu, b, length, s);
+        const double2 *B = static_cast<const double2 *>(b_in);
+        const void *before[3] = {bt->ta.p, bt->partial.p, bt->hx.p};
+        int rc = prepare_general(bt, B, b, s);
+        if (rc) return rc;
+        const void *after[3] = {bt->ta.p, bt->partial.p, bt->hx.p};
+        if (!std::equal(before, before + 3, after)) {  // recorded graphs point at the old buffers
+            for (auto &kv : bt->graphs) cudaGraphExecDestroy(kv.second);
+            bt->graphs.clear();
+        }
+        auto rec = [&](cudaStream_t st) {
+            return m == 1 ? record_general<1>(bt, B, mu, b, length, st) : record_general<2>(bt, B, mu, b, length, st);
+        };
+        if (!use_graph) {
+            if ((rc = rec(s))) return rc;
+            return general_status(bt, s);
+        }
+        // one graph for the whole call: every solve is a WHILE node inside it
+        const auto key = std::make_tuple((const void *)B, (const void *)mu, b, length, 2, bt->tiles.tile_rows);
+        auto it = bt->graphs.find(key);
+        if (it == bt->graphs.end()) {
+            if (!bt->cap) KMSD_CUDA(cudaStreamCreateWithFlags(&bt->cap, cudaStreamNonBlocking));
+            // the SpMMs size this thread's reduction buffers on first use:
+            // run them once outside the capture
+            if ((rc = spmm64(bt->gm->S, B, bt->t1.as<double2>(), b, s))) return rc;
+            if ((rc = spmm64(bt->gh, B, bt->t1.as<double2>(), b, s))) return rc;
+            KMSD_CUDA(cudaStreamSynchronize(s));
+            cudaGraph_t g = nullptr;
+            int64_t recorded = 0;
+            {
+                CountOff off;
+                KMSD_CUDA(cudaStreamBeginCapture(bt->cap, cudaStreamCaptureModeThreadLocal));
+                rc = rec(bt->cap);
+                const cudaError_t e = cudaStreamEndCapture(bt->cap, &g);
+                recorded = off.recorded();
+                if (rc) {
+                    if (g) cudaGraphDestroy(g);
+                    return rc;
+                }
+                if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture (nonorthogonal batch)");
+            }
+            cudaGraphExec_t exec;
+            const cudaError_t ei = cudaGraphInstantiate(&exec, g, 0);
+            cudaGraphDestroy(g);
+            if (ei != cudaSuccess) return cuda_fail(ei, "cudaGraphInstantiate (nonorthogonal batch)");
+            it = bt->graphs.emplace(key, exec).first;
+            bt->general_kernels = recorded;
+        }
+        KMSD_CUDA(cudaGraphLaunch(it->second, s));
+        count_launch(bt->general_kernels);  // the PCG loop bodies are counted on the device
+        return general_status(bt, s);
     }
     int rc = bt->precision == KMSD_MIXED
                  ? run_batch<float>(bt, static_cast<const double2 *>(b_in), mu, b, length, doubling, s, use_graph)

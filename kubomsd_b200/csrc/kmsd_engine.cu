@@ -60,7 +60,15 @@ void DevBuf::release() {
     bytes = 0;
 }
 static std::atomic<int64_t> g_launches{0};
-void count_launch(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+static thread_local int g_count_off = 0;
+static thread_local int64_t g_recorded = 0;
+void count_launch(int64_t n) {
+    if (g_count_off) g_recorded += n;
+    else g_launches.fetch_add(n, std::memory_order_relaxed);
+}
+CountOff::CountOff() : start(g_recorded) { ++g_count_off; }
+CountOff::~CountOff() { --g_count_off; }
+int64_t CountOff::recorded() const { return g_recorded - start; }
 int64_t launches() { return g_launches.load(std::memory_order_relaxed); }
 int sm_count() {
     static int cached = 0;
@@ -321,7 +329,7 @@ extern "C" {
 
 const char *kmsd_last_error(void) { return g_last_error.c_str(); }
 
-int64_t kmsd_kernel_launches(void) { return launches(); }
+int64_t kmsd_kernel_launches(void) { return launches() + device_loop_launches(); }
 
 const char *kmsd_build_info(void) {
     return "{\"language\": \"C++17/CUDA\", \"architecture\": \"sm_100a\", "

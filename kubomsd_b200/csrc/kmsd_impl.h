@@ -37,6 +37,18 @@ struct DevBuf {
 int sm_count();
 // Process-wide count of kernels launched by the library.
 void count_launch(int64_t n = 1);
+// While a CountOff lives, this thread's launches are tallied instead of
+// counted: launches recorded into a graph during capture are counted each
+// time the graph runs (recorded() of them per launch).
+struct CountOff {
+    CountOff();
+    ~CountOff();
+    int64_t recorded() const;
+    int64_t start;
+};
+// Kernels launched by device-driven loops on the current device (read from
+// the device; synchronises it).
+int64_t device_loop_launches();
 // Grid for a row-group kernel over `rows` rows.
 int grid_for(int64_t rows, const RowMap &mp);
 // Grid of one resident wave of `kernel` (occupancy API; cached per kernel and
@@ -144,6 +156,19 @@ struct kmsd_metric_s {
     bool seg_aligned4 = false;  // every segment starts on a multiple of 4 rows
     std::map<int, SegPlan> seg_plans;
     int seg_plan(int gpc, SegPlan **out);
+    // Whole solves captured as graphs with a device-driven iteration loop,
+    // per argument set; valid while the workspace pointers in graph_ws hold.
+    cudaStream_t loop_stream = nullptr, check_stream = nullptr, cap_stream = nullptr;
+    std::map<std::vector<uint64_t>, std::pair<cudaGraphExec_t, int64_t>> graphs;  // exec, kernels recorded
+    std::vector<const void *> graph_ws;
+    // The same solve as `solve` (asynchronous form), with the iterations
+    // driven by the device: one graph launch per call, no host polling.
+    // When `s` is capturing, the solve is recorded into that capture.
+    int solve_dev(const double2 *B, double2 *Y, int64_t b, double rtol, double atol, int maxiter, cudaStream_t s,
+                  int *status, void *fail_report);
+    // Allocates everything a device-driven solve of b columns needs, so that
+    // a later capture allocates nothing.
+    int prepare_dev(int64_t b);
     // state_cols: per-column state entries (nseg * b for a segmented solve)
     int ensure(int64_t b, int64_t state_cols = 0);
     // Batched PCG on device buffers (complex128).  When `report` is null and

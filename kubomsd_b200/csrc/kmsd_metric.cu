@@ -415,11 +415,31 @@ __device__ __forceinline__ void for_rows_spmv(const CsrView<double> &S, const Bs
     }
 }
 
+// Device-driven iterations: the solve is captured with its iterations as a
+// WHILE node (`again`) whose body holds an IF node (`check`) around the
+// true-residual and restart kernels.  The update kernel's last CTA counts
+// the iteration in flags[5] and sets both conditions; the restart kernel's
+// last CTA decides `again` after a check; an update that finds the halt
+// word stops the loop.  on == 0: iterations driven by the host.
+struct Loop {
+    int on, maxiter;
+    cudaGraphConditionalHandle again, check;
+};
+
+// Kernels launched inside device-driven loops, counted on the device (the
+// host does not see those launches).
+__device__ unsigned long long g_loop_launches;
+
+__device__ __forceinline__ void loop_count(const Loop &lp) {
+    if (lp.on && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&g_loop_launches, 1ull);
+}
+
 // ---- sp = S p, curvature <p, sp>, alpha, breakdown
 template <int MU, int SF, bool SEG>
 __global__ void __launch_bounds__(256)
     pcg_spmv_kernel(CsrView<double> S, BsrView<double> SB, const double2 *p, double2 *sp, int64_t n, RowMap mp,
-                    ColPtr c, double2 *partial, Ticket *tk, SegView sv) {
+                    ColPtr c, double2 *partial, Ticket *tk, SegView sv, Loop lp) {
+    loop_count(lp);
     if (*(volatile int *)c.flags) return;
     extern __shared__ double2 smem[];
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
@@ -475,8 +495,13 @@ __global__ void __launch_bounds__(256)
 template <int MU, int MAXB, bool SEG>
 __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
     pcg_update_kernel(double2 *y, double2 *r, double2 *z, const double2 *p, const double2 *sp, Pre P, int64_t nb,
-                      RowMap mp, ColPtr c, int refresh, int adaptive, double2 *partial, Ticket *tk, SegView sv) {
-    if (*(volatile int *)c.flags) return;
+                      RowMap mp, ColPtr c, int refresh, int interval, int adaptive, double2 *partial, Ticket *tk,
+                      SegView sv, Loop lp) {
+    loop_count(lp);
+    if (*(volatile int *)c.flags) {
+        if (lp.on && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(lp.again, 0u);
+        return;
+    }
     extern __shared__ double2 smem[];
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
     const int U = mp.U;
@@ -536,6 +561,8 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
             cand = act && rn <= c.thr[cj];
         }
         const bool candidate = __syncthreads_or(cand);
+        // in a device-driven loop the iteration index lives in flags[5]
+        if (interval > 0) refresh = ((*(volatile int *)(c.flags + 5) + 1) % interval) == 0;
         const bool check = refresh || (adaptive && candidate);
         bool act_now = false;
         if (j < U) {
@@ -572,6 +599,12 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
                 c.flags[4] = total;
                 if (!any && total == 0) c.flags[0] = 1;
             }
+            if (lp.on) {
+                const int k = c.flags[5] + 1;
+                c.flags[5] = k;
+                cudaGraphSetConditional(lp.check, c.flags[1] ? 1u : 0u);
+                cudaGraphSetConditional(lp.again, (c.flags[0] == 0 && k < lp.maxiter) ? 1u : 0u);
+            }
         }
     }
 }
@@ -581,7 +614,8 @@ template <int MU, int SF, bool SEG>
 __global__ void __launch_bounds__(256)
     pcg_true_residual_kernel(CsrView<double> S, BsrView<double> SB, const double2 *q, const double2 *y,
                              const double2 *r, double2 *t, int64_t n, RowMap mp, ColPtr c, int adaptive,
-                             double gap_ratio, double2 *partial, Ticket *tk, Counters *cnt, SegView sv) {
+                             double gap_ratio, double2 *partial, Ticket *tk, Counters *cnt, SegView sv, Loop lp) {
+    loop_count(lp);
     if (*(volatile int *)c.flags || !*(volatile int *)(c.flags + 1)) return;
     extern __shared__ double2 smem[];
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
@@ -649,7 +683,8 @@ __global__ void __launch_bounds__(256)
 template <int MU, int MAXB, bool SEG>
 __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
     pcg_restart_kernel(double2 *r, double2 *z, const double2 *t, Pre P, int64_t nb, RowMap mp, ColPtr c,
-                       double2 *partial, Ticket *tk, SegView sv) {
+                       double2 *partial, Ticket *tk, SegView sv, Loop lp) {
+    loop_count(lp);
     if (*(volatile int *)c.flags || !*(volatile int *)(c.flags + 1)) return;
     extern __shared__ double2 smem[];
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
@@ -716,6 +751,7 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
             c.flags[1] = 0;
             c.flags[4] = total;
             if (total == 0) c.flags[0] = 1;
+            if (lp.on) cudaGraphSetConditional(lp.again, (c.flags[0] == 0 && c.flags[5] < lp.maxiter) ? 1u : 0u);
         }
     }
 }
@@ -728,7 +764,9 @@ __device__ __forceinline__ double2 direction(const ColPtr &c, size_t cj, double2
     return make_double2(zv.x + pv.x * be, zv.y + pv.y * be);
 }
 template <bool SEG>
-__global__ void pcg_direction_kernel(const double2 *z, double2 *p, int64_t len, RowMap mp, ColPtr c, SegView sv) {
+__global__ void pcg_direction_kernel(const double2 *z, double2 *p, int64_t len, RowMap mp, ColPtr c, SegView sv,
+                                     Loop lp) {
+    loop_count(lp);
     if (*(volatile int *)c.flags) return;
     if constexpr (!SEG) {
         const int U = mp.U;
@@ -981,9 +1019,14 @@ int kmsd_metric_s::seg_plan(int gpc, SegPlan **out) {
 
 namespace {
 
+// How run_pcg drives the iterations: from the host (polling the halt word),
+// not at all (only the workspace is prepared, so that a capture allocates
+// nothing), or from the device as the WHILE node of a capturing stream.
+enum { kHostLoop = 0, kPrepare = 1, kDeviceLoop = 2 };
+
 template <int MU, int MAXB, int SF, bool SEG>
 int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rtol, double atol, int maxiter,
-            cudaStream_t s, int *status, FailReportFull *fr, int *claimed) {
+            cudaStream_t s, int *status, FailReportFull *fr, int *claimed, int mode) {
     const int64_t n = M->n;
     const RowMap mp = make_map((int)b, kThreads);
     const int64_t nb = MAXB == 1 ? n : M->nblocks;
@@ -1011,6 +1054,7 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
         if (M->red.ensure(std::max(grid_r, std::max(grid_b, grid_s)), (int)b)) return KMSD_ECUDA;
         tk = M->red.tick();
     }
+    if (mode == kPrepare) return KMSD_OK;
     const int64_t ncols = (int64_t)sv.nseg * b;
     ColPtr c = col_ptr(M->cols.p, ncols);
     Pre P{M->diag, M->bstart, M->foff, M->factors, M->ub};
@@ -1028,35 +1072,103 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
     count_launch();
     pcg_pinit_kernel<SEG><<<egrid, 256, 0, s>>>(z, p, len, mp, c, sv);
     count_launch();
-    volatile int *hflag = static_cast<volatile int *>(M->host_pinned.p);
-    const int chunk = 4;
-    int slot = 0, pending = 0;
-    for (int k = 0; k < maxiter; ++k) {
-        const int refresh = ((k + 1) % M->interval) == 0;
-        pcg_spmv_kernel<MU, SF, SEG><<<grid_s, kThreads, sm, s>>>(S, SB, p, sp, n, mp, c, part, tk, sv);
-        count_launch();
-        pcg_update_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, s>>>(y, r, z, p, sp, P, nb, mp, c, refresh,
-                                                                      M->adaptive, part, tk, sv);
-        count_launch();
-        if (refresh || M->adaptive) {
-            pcg_true_residual_kernel<MU, SF, SEG><<<grid_s, kThreads, sm, s>>>(
-                S, SB, q, y, r, t, n, mp, c, M->adaptive, M->gap_ratio, part, tk, cnt, sv);
-            count_launch();
-            pcg_restart_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, s>>>(r, z, t, P, nb, mp, c, part, tk, sv);
-            count_launch();
+    if (mode == kDeviceLoop) {
+        // The iterations as a WHILE node of the capture on s.  Its body is
+        // captured on the metric's loop stream: spmv, update, an IF node
+        // (captured on the check stream) around the true residual and the
+        // restart, and the direction.
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t nd = 0;
+        KMSD_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+        if (cs != cudaStreamCaptureStatusActive) return fail(KMSD_ERUNTIME, "a device-driven PCG loop must be captured");
+        // (the node parameters' union has no default constructor)
+        alignas(cudaGraphNodeParams) unsigned char w_store[sizeof(cudaGraphNodeParams)] = {};
+        alignas(cudaGraphNodeParams) unsigned char i_store[sizeof(cudaGraphNodeParams)] = {};
+        cudaGraphNodeParams &wp = *reinterpret_cast<cudaGraphNodeParams *>(w_store);
+        cudaGraphNodeParams &ip = *reinterpret_cast<cudaGraphNodeParams *>(i_store);
+        Loop lp{1, maxiter, 0, 0};
+        KMSD_CUDA(cudaGraphConditionalHandleCreate(&lp.again, g, 1, cudaGraphCondAssignDefault));
+        wp.type = cudaGraphNodeTypeConditional;
+        wp.conditional.handle = lp.again;
+        wp.conditional.type = cudaGraphCondTypeWhile;
+        wp.conditional.size = 1;
+        cudaGraphNode_t wnode;
+        KMSD_CUDA(cudaGraphAddNode(&wnode, g, deps, nd, &wp));
+        KMSD_CUDA(cudaStreamUpdateCaptureDependencies(s, &wnode, 1, cudaStreamSetCaptureDependencies));
+        cudaGraph_t body = wp.conditional.phGraph_out[0];
+        KMSD_CUDA(cudaGraphConditionalHandleCreate(&lp.check, body, 0, cudaGraphCondAssignDefault));
+        cudaStream_t bs = M->loop_stream, cs2 = M->check_stream;
+        KMSD_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        pcg_spmv_kernel<MU, SF, SEG><<<grid_s, kThreads, sm, bs>>>(S, SB, p, sp, n, mp, c, part, tk, sv, lp);
+        pcg_update_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, bs>>>(y, r, z, p, sp, P, nb, mp, c, 0, M->interval,
+                                                                       M->adaptive, part, tk, sv, lp);
+        cudaError_t le = cudaGetLastError();
+        cudaStreamCaptureStatus bcs;
+        cudaGraph_t bg = nullptr;
+        const cudaGraphNode_t *bdeps = nullptr;
+        size_t bnd = 0;
+        cudaGraphNode_t inode = nullptr;
+        cudaError_t ae = cudaStreamGetCaptureInfo(bs, &bcs, nullptr, &bg, &bdeps, &bnd);
+        if (ae == cudaSuccess) {
+            ip.type = cudaGraphNodeTypeConditional;
+            ip.conditional.handle = lp.check;
+            ip.conditional.type = cudaGraphCondTypeIf;
+            ip.conditional.size = 1;
+            ae = cudaGraphAddNode(&inode, bg, bdeps, bnd, &ip);
         }
-        pcg_direction_kernel<SEG><<<egrid, 256, 0, s>>>(z, p, len, mp, c, sv);
-        count_launch();
-        if ((k + 1) % chunk == 0) {
-            KMSD_CUDA(cudaMemcpyAsync((void *)(hflag + slot), c.flags, sizeof(int), cudaMemcpyDeviceToHost, s));
-            KMSD_CUDA(cudaEventRecord(M->ev[slot], s));
-            ++pending;
-            const int other = slot ^ 1;
-            if (pending >= 2) {
-                KMSD_CUDA(cudaEventSynchronize(M->ev[other]));
-                if (hflag[other]) break;
+        if (ae == cudaSuccess) ae = cudaStreamUpdateCaptureDependencies(bs, &inode, 1, cudaStreamSetCaptureDependencies);
+        if (ae == cudaSuccess)
+            ae = cudaStreamBeginCaptureToGraph(cs2, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal);
+        if (ae == cudaSuccess) {
+            pcg_true_residual_kernel<MU, SF, SEG><<<grid_s, kThreads, sm, cs2>>>(
+                S, SB, q, y, r, t, n, mp, c, M->adaptive, M->gap_ratio, part, tk, cnt, sv, lp);
+            pcg_restart_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, cs2>>>(r, z, t, P, nb, mp, c, part, tk, sv, lp);
+            if (le == cudaSuccess) le = cudaGetLastError();
+            cudaGraph_t ib = nullptr;
+            ae = cudaStreamEndCapture(cs2, &ib);
+        }
+        pcg_direction_kernel<SEG><<<egrid, 256, 0, bs>>>(z, p, len, mp, c, sv, lp);
+        if (le == cudaSuccess) le = cudaGetLastError();
+        cudaGraph_t bout = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(bs, &bout);
+        if (ae != cudaSuccess) return cuda_fail(ae, "device PCG loop (check branch)");
+        if (le != cudaSuccess) return cuda_fail(le, "device PCG loop body");
+        if (ee != cudaSuccess) return cuda_fail(ee, "cudaStreamEndCapture (device PCG loop body)");
+    } else {
+        volatile int *hflag = static_cast<volatile int *>(M->host_pinned.p);
+        const int chunk = 4;
+        int slot = 0, pending = 0;
+        for (int k = 0; k < maxiter; ++k) {
+            const int refresh = ((k + 1) % M->interval) == 0;
+            pcg_spmv_kernel<MU, SF, SEG><<<grid_s, kThreads, sm, s>>>(S, SB, p, sp, n, mp, c, part, tk, sv, Loop{});
+            count_launch();
+            pcg_update_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, s>>>(y, r, z, p, sp, P, nb, mp, c, refresh, 0,
+                                                                          M->adaptive, part, tk, sv, Loop{});
+            count_launch();
+            if (refresh || M->adaptive) {
+                pcg_true_residual_kernel<MU, SF, SEG><<<grid_s, kThreads, sm, s>>>(
+                    S, SB, q, y, r, t, n, mp, c, M->adaptive, M->gap_ratio, part, tk, cnt, sv, Loop{});
+                count_launch();
+                pcg_restart_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, s>>>(r, z, t, P, nb, mp, c, part, tk, sv,
+                                                                               Loop{});
+                count_launch();
             }
-            slot = other;
+            pcg_direction_kernel<SEG><<<egrid, 256, 0, s>>>(z, p, len, mp, c, sv, Loop{});
+            count_launch();
+            if ((k + 1) % chunk == 0) {
+                KMSD_CUDA(cudaMemcpyAsync((void *)(hflag + slot), c.flags, sizeof(int), cudaMemcpyDeviceToHost, s));
+                KMSD_CUDA(cudaEventRecord(M->ev[slot], s));
+                ++pending;
+                const int other = slot ^ 1;
+                if (pending >= 2) {
+                    KMSD_CUDA(cudaEventSynchronize(M->ev[other]));
+                    if (hflag[other]) break;
+                }
+                slot = other;
+            }
         }
     }
     KMSD_CUDA(cudaGetLastError());
@@ -1073,7 +1185,7 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
 }
 
 using PcgFn = int (*)(kmsd_metric_s *, const double2 *, double2 *, int64_t, double, double, int, cudaStream_t,
-                      int *, FailReportFull *, int *);
+                      int *, FailReportFull *, int *, int);
 
 template <int MAXB, int SF, bool SEG>
 PcgFn pick_mu(int mu) {
@@ -1132,7 +1244,7 @@ int kmsd_metric_s::solve(const double2 *B, double2 *Y, int64_t b, double rtol, d
         KMSD_CUDA(cudaMemsetAsync(st, 0, 2 * sizeof(int), s));
     }
     claimed = st + 1;
-    int rc = fn(this, B, Y, b, rtol, atol, maxiter, s, st, fr, claimed);
+    int rc = fn(this, B, Y, b, rtol, atol, maxiter, s, st, fr, claimed, kHostLoop);
     if (rc) return rc;
     ++calls;
     if (!sync) return KMSD_OK;
@@ -1173,6 +1285,110 @@ int kmsd_metric_s::solve(const double2 *B, double2 *Y, int64_t b, double rtol, d
         if (flags[3]) return fail(KMSD_EMETRIC, "PCG non-positive/complex curvature breakdown");
         return fail(KMSD_EMETRIC, "S solve failed true-residual acceptance");
     }
+    return KMSD_OK;
+}
+
+namespace kmsd {
+int64_t device_loop_launches() {
+    unsigned long long v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_loop_launches, sizeof(v)) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return (int64_t)v;
+}
+}  // namespace kmsd
+
+int kmsd_metric_s::prepare_dev(int64_t b) {
+    if (b < 1 || b > 256) return fail(KMSD_EINVAL, "metric solve supports at most 256 columns per call");
+    const bool seg = nseg > 1;
+    if (ensure(b, seg ? nseg * b : b)) return KMSD_ECUDA;
+    const RowMap mp = make_map((int)b, kThreads);
+    const bool bsr = S->bsr_nb > 0 && (!seg || seg_aligned4);
+    const int sf = bsr ? (S->bsr64().im ? S_BSR_CPLX : S_BSR_REAL) : S_CSR;
+    PcgFn fn = pick(mu_for(mp), nblocks ? maxb : 1, sf, seg);
+    if (!fn) return fail(KMSD_EINVAL, "unsupported metric block size / column count");
+    if (!loop_stream) KMSD_CUDA(cudaStreamCreateWithFlags(&loop_stream, cudaStreamNonBlocking));
+    if (!check_stream) KMSD_CUDA(cudaStreamCreateWithFlags(&check_stream, cudaStreamNonBlocking));
+    return fn(this, nullptr, nullptr, b, 0., 0., 1, nullptr, nullptr, nullptr, nullptr, kPrepare);
+}
+
+int kmsd_metric_s::solve_dev(const double2 *B, double2 *Y, int64_t b, double rtol, double atol, int maxiter,
+                             cudaStream_t s, int *status, void *fail_report) {
+    if (b < 1 || !std::isfinite(rtol) || !std::isfinite(atol) || rtol < 0 || atol < 0 || maxiter < 1)
+        return fail(KMSD_EINVAL, "invalid metric RHS shape/tolerances");
+    if (b > 256) return fail(KMSD_EINVAL, "metric solve supports at most 256 columns per call");
+    if (!status || !fail_report) return fail(KMSD_EINVAL, "a device-driven solve reports through a status word");
+    const bool seg = nseg > 1;
+    const int64_t ncols = seg ? nseg * b : b;
+    if (ensure(b, ncols)) return KMSD_ECUDA;
+    const RowMap mp = make_map((int)b, kThreads);
+    const bool bsr = S->bsr_nb > 0 && (!seg || seg_aligned4);
+    const int sf = bsr ? (S->bsr64().im ? S_BSR_CPLX : S_BSR_REAL) : S_CSR;
+    PcgFn fn = pick(mu_for(mp), nblocks ? maxb : 1, sf, seg);
+    if (!fn) return fail(KMSD_EINVAL, "unsupported metric block size / column count");
+    if (!loop_stream) KMSD_CUDA(cudaStreamCreateWithFlags(&loop_stream, cudaStreamNonBlocking));
+    if (!check_stream) KMSD_CUDA(cudaStreamCreateWithFlags(&check_stream, cudaStreamNonBlocking));
+    FailReportFull *fr = static_cast<FailReportFull *>(fail_report);
+    int *claimed = status + 1;
+    // every allocation happens here, outside any capture
+    int rc = fn(this, B, Y, b, rtol, atol, maxiter, s, status, fr, claimed, kPrepare);
+    if (rc) return rc;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    KMSD_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (cs == cudaStreamCaptureStatusActive) {  // part of the caller's graph
+        CountOff off;
+        rc = fn(this, B, Y, b, rtol, atol, maxiter, s, status, fr, claimed, kDeviceLoop);
+        if (!rc) ++calls;
+        return rc;
+    }
+    // the workspace the cached graphs point into
+    std::vector<const void *> ws = {q.p, y.p, r.p, z.p, p.p, sp.p, t.p, cols.p, dcount.p, red.partial.p, red.ticket.p};
+    for (auto &kv : seg_plans) ws.push_back(kv.second.mem.p);
+    if (ws != graph_ws) {
+        for (auto &kv : graphs) cudaGraphExecDestroy(kv.second.first);
+        graphs.clear();
+        graph_ws = ws;
+    }
+    auto bits = [](double x) {
+        uint64_t u;
+        std::memcpy(&u, &x, sizeof(u));
+        return u;
+    };
+    const std::vector<uint64_t> key = {(uint64_t)(uintptr_t)B, (uint64_t)(uintptr_t)Y, (uint64_t)b, bits(rtol),
+                                       bits(atol), (uint64_t)maxiter, (uint64_t)(uintptr_t)status,
+                                       (uint64_t)(uintptr_t)fail_report, (uint64_t)adaptive, (uint64_t)interval,
+                                       bits(gap_ratio)};
+    auto it = graphs.find(key);
+    if (it == graphs.end()) {
+        if (graphs.size() >= 32) {  // bounded cache
+            for (auto &kv : graphs) cudaGraphExecDestroy(kv.second.first);
+            graphs.clear();
+        }
+        if (!cap_stream) KMSD_CUDA(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        int64_t recorded = 0;
+        {
+            CountOff off;
+            KMSD_CUDA(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal));
+            rc = fn(this, B, Y, b, rtol, atol, maxiter, cap_stream, status, fr, claimed, kDeviceLoop);
+            const cudaError_t e = cudaStreamEndCapture(cap_stream, &g);
+            recorded = off.recorded();
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture (device PCG solve)");
+        }
+        cudaGraphExec_t exec;
+        const cudaError_t ei = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) return cuda_fail(ei, "cudaGraphInstantiate (device PCG solve)");
+        it = graphs.emplace(key, std::make_pair(exec, recorded)).first;
+    }
+    KMSD_CUDA(cudaGraphLaunch(it->second.first, s));
+    count_launch(it->second.second);  // the loop body's kernels are counted on the device
+    ++calls;
     return KMSD_OK;
 }
 
@@ -1308,6 +1524,10 @@ void kmsd_metric_destroy(kmsd_metric m) {
     m->red.ticket.release();
     if (m->host_pinned.p) cudaFreeHost(m->host_pinned.p);
     for (auto &kv : m->seg_plans) kv.second.mem.release();
+    for (auto &kv : m->graphs) cudaGraphExecDestroy(kv.second.first);
+    if (m->loop_stream) cudaStreamDestroy(m->loop_stream);
+    if (m->check_stream) cudaStreamDestroy(m->check_stream);
+    if (m->cap_stream) cudaStreamDestroy(m->cap_stream);
     for (auto &e : m->ev)
         if (e) cudaEventDestroy(e);
     delete m;

@@ -70,7 +70,7 @@ int solve(E *e, const double2 *B, double2 *Y, int64_t b, const Ctl &c, cudaStrea
         e->M->calls += 1;
         return KMSD_OK;
     }
-    return e->M->solve(B, Y, b, c.rtol, c.atol, c.maxiter, nullptr, s, status_ptr(e), e->report.p);
+    return e->M->solve_dev(B, Y, b, c.rtol, c.atol, c.maxiter, s, status_ptr(e), e->report.p);
 }
 
 // out = S^-1 H B

@@ -134,7 +134,10 @@ def test_nonorthogonal_batch_equals_each_instance(cuda):
     phases = [kpm.random_phases(H.shape[0], 11 + i, range(8)) for i, (H, _, _) in enumerate(models)]
     bt = B200Batch([m[0] for m in models], precision="fp64", tile_rows=64, overlaps=[m[1] for m in models],
                    blocks=[m[2] for m in models], rtol=1e-12)
-    got = bt.moments(phases, 40, c, a).cpu().numpy()
+    B = bt.concat(phases)
+    got = bt.moments(B, 40, c, a).cpu().numpy()  # captured: every solve a device-driven loop
+    np.testing.assert_array_equal(bt.moments(B, 40, c, a).cpu().numpy(), got)  # graph replay
+    np.testing.assert_array_equal(bt.moments(B, 40, c, a, use_graph=False).cpu().numpy(), got)
     for i, (H, S, blocks) in enumerate(models):
         eng = O.engine_from_model(H, S, blocks=blocks, rtol=1e-12)
         want = eng.moments(phases[i], 40, c[i], a[i])
