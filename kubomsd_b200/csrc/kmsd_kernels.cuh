@@ -109,16 +109,19 @@ __device__ __forceinline__ void gather_row_ell(const EllView<T> &A, const typena
 // selects complex block values at compile time, so a real matrix (the usual
 // tight-binding S and H) carries no registers for imaginary parts; block
 // values are loaded one block row at a time.
+// With ks > 1 this call takes only the blocks part, part + ks, ... of the
+// block row (a split of one block row over ks row groups).
 template <int MU, bool CPLX>
 __device__ __forceinline__ void gather_block_row(const BsrView<double> &A, const double2 *X, int64_t I, int U,
-                                                 int G, int lane, Pk<double> (&acc)[4][MU]) {
-    const int k0 = __ldg(A.bptr + I), k1 = __ldg(A.bptr + I + 1);
+                                                 int G, int lane, Pk<double> (&acc)[4][MU], int part = 0,
+                                                 int ks = 1) {
+    const int k0 = __ldg(A.bptr + I) + part, k1 = __ldg(A.bptr + I + 1);
     // the next block's column index is loaded one block ahead, so each
     // block's gathers wait for one memory round trip, not two
     int Jn = k0 < k1 ? __ldg(A.bidx + k0) : 0;
-    for (int k = k0; k < k1; ++k) {
+    for (int k = k0; k < k1; k += ks) {
         const int J = Jn;
-        if (k + 1 < k1) Jn = __ldg(A.bidx + k + 1);
+        if (k + ks < k1) Jn = __ldg(A.bidx + k + ks);
         Pk<double> x[MU][4];
 #pragma unroll
         for (int m = 0; m < MU; ++m) {

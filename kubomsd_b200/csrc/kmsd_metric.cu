@@ -390,10 +390,57 @@ enum { S_CSR = 0, S_BSR_REAL = 1, S_BSR_CPLX = 2 };
 // Calls f(row, yv) for every row of rows [x.r0, x.r1) owned by this thread's
 // row group, with yv[m] = (S X)[row, unit lane + m*G], from CSR or from 4x4
 // blocks (a block row's four rows share every gathered input row).
+//
+// Small operators (few block rows for the resident row groups) split each
+// block row over ks row groups of the CTA: group g takes every ks-th block,
+// which divides the chain of dependent gathers by ks, and the partials are
+// summed in shared memory in a fixed order before f.  Every thread of the CTA
+// calls this when ks > 1 (the split synchronises the CTA); the dynamic shared
+// memory then holds split_smem_units(MU) double2.
+__host__ __device__ constexpr int split_smem_units(int mu) { return 1024 * mu; }
+
 template <int MU, int SF, class F>
 __device__ __forceinline__ void for_rows_spmv(const CsrView<double> &S, const BsrView<double> &SB, const double2 *X,
-                                              const Ctx &x, const RowMap &mp, int g, int lane, F &&f) {
-    if constexpr (SF != S_CSR) {
+                                              const Ctx &x, const RowMap &mp, int g, int lane, int ks, F &&f) {
+    if (SF != S_CSR && ks > 1) {
+        extern __shared__ double2 part_sums[];  // [group][4 rows][MU][G lanes]
+        const int spc = mp.gpc / ks, slot = g / ks, part = g % ks;
+        const int64_t end = x.r1 / 4;
+        for (int64_t base = x.r0 / 4 + (int64_t)x.lc * spc; base < end; base += (int64_t)x.nct * spc) {
+            const int64_t I = base + slot;
+            Pk<double> acc4[4][MU];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int m = 0; m < MU; ++m) acc4[i][m] = pk_zero<double>();
+            if (I < end) gather_block_row<MU, SF == S_BSR_CPLX>(SB, X, I, mp.U, mp.G, lane, acc4, part, ks);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int m = 0; m < MU; ++m)
+                    part_sums[((g * 4 + i) * MU + m) * mp.G + lane] = make_double2(acc4[i][m].re[0], acc4[i][m].im[0]);
+            __syncthreads();
+            if (part == 0 && I < end) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    Pk<double> yv[MU];
+#pragma unroll
+                    for (int m = 0; m < MU; ++m) {
+                        double re = 0., im = 0.;
+                        for (int q = 0; q < ks; ++q) {
+                            const double2 v = part_sums[(((g + q) * 4 + i) * MU + m) * mp.G + lane];
+                            re += v.x;
+                            im += v.y;
+                        }
+                        yv[m].re[0] = re;
+                        yv[m].im[0] = im;
+                    }
+                    f(4 * I + i, yv);
+                }
+            }
+            __syncthreads();
+        }
+    } else if constexpr (SF != S_CSR) {
         for (int64_t I = x.r0 / 4 + (int64_t)x.lc * mp.gpc + g; I < x.r1 / 4; I += (int64_t)x.nct * mp.gpc) {
             Pk<double> acc4[4][MU];
 #pragma unroll
@@ -438,7 +485,7 @@ __device__ __forceinline__ void loop_count(const Loop &lp) {
 template <int MU, int SF, bool SEG>
 __global__ void __launch_bounds__(256)
     pcg_spmv_kernel(CsrView<double> S, BsrView<double> SB, const double2 *p, double2 *sp, int64_t n, RowMap mp,
-                    ColPtr c, double2 *partial, Ticket *tk, SegView sv, Loop lp) {
+                    ColPtr c, double2 *partial, Ticket *tk, SegView sv, Loop lp, int ks) {
     loop_count(lp);
     if (*(volatile int *)c.flags) return;
     extern __shared__ double2 smem[];
@@ -446,7 +493,7 @@ __global__ void __launch_bounds__(256)
     const Ctx x = seg_ctx<SEG>(sv, n, 0);
     double2 acc[MU][1];
     ZERO_ACC(acc);
-    for_rows_spmv<MU, SF>(S, SB, p, x, mp, g, lane, [&](int64_t row, const Pk<double>(&yv)[MU]) {
+    for_rows_spmv<MU, SF>(S, SB, p, x, mp, g, lane, ks, [&](int64_t row, const Pk<double>(&yv)[MU]) {
 #pragma unroll
         for (int m = 0; m < MU; ++m) {
             const int u = lane + m * mp.G;
@@ -614,7 +661,8 @@ template <int MU, int SF, bool SEG>
 __global__ void __launch_bounds__(256)
     pcg_true_residual_kernel(CsrView<double> S, BsrView<double> SB, const double2 *q, const double2 *y,
                              const double2 *r, double2 *t, int64_t n, RowMap mp, ColPtr c, int adaptive,
-                             double gap_ratio, double2 *partial, Ticket *tk, Counters *cnt, SegView sv, Loop lp) {
+                             double gap_ratio, double2 *partial, Ticket *tk, Counters *cnt, SegView sv, Loop lp,
+                             int ks) {
     loop_count(lp);
     if (*(volatile int *)c.flags || !*(volatile int *)(c.flags + 1)) return;
     extern __shared__ double2 smem[];
@@ -625,7 +673,7 @@ __global__ void __launch_bounds__(256)
     double2 acc[MU][1];
     ZERO_ACC(acc);
     if (due) {
-        for_rows_spmv<MU, SF>(S, SB, y, x, mp, g, lane, [&](int64_t row, const Pk<double>(&sy)[MU]) {
+        for_rows_spmv<MU, SF>(S, SB, y, x, mp, g, lane, ks, [&](int64_t row, const Pk<double>(&sy)[MU]) {
 #pragma unroll
             for (int m = 0; m < MU; ++m) {
                 const int u = lane + m * mp.G;
@@ -795,13 +843,13 @@ __global__ void pcg_direction_kernel(const double2 *z, double2 *p, int64_t len, 
 template <int MU, int SF, bool SEG>
 __global__ void __launch_bounds__(256)
     pcg_final_kernel(CsrView<double> S, BsrView<double> SB, const double2 *q, const double2 *y, int64_t n,
-                     RowMap mp, ColPtr c, double2 *partial, Ticket *tk, Counters *cnt, SegView sv) {
+                     RowMap mp, ColPtr c, double2 *partial, Ticket *tk, Counters *cnt, SegView sv, int ks) {
     extern __shared__ double2 smem[];
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
     const Ctx x = seg_ctx<SEG>(sv, n, 0);
     double2 acc[MU][1];
     ZERO_ACC(acc);
-    for_rows_spmv<MU, SF>(S, SB, y, x, mp, g, lane, [&](int64_t row, const Pk<double>(&sy)[MU]) {
+    for_rows_spmv<MU, SF>(S, SB, y, x, mp, g, lane, ks, [&](int64_t row, const Pk<double>(&sy)[MU]) {
 #pragma unroll
         for (int m = 0; m < MU; ++m) {
             const int u = lane + m * mp.G;
@@ -1032,6 +1080,15 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
     const int64_t nb = MAXB == 1 ? n : M->nblocks;
     const BsrView<double> SB = M->S->bsr64();
     const size_t sm = reduce_smem(mp, 1);
+    // split each 4x4 block row over ks row groups while there are few block
+    // rows for the resident row groups (four CTAs per SM)
+    int ks = 1;
+    if constexpr (SF != S_CSR) {
+        const int64_t resident = (int64_t)sm_count() * 4 * mp.gpc;
+        const int kmax = std::min(8, mp.gpc);
+        while (ks * 2 <= kmax && M->S->bsr_nb * ks * 2 <= resident) ks *= 2;
+    }
+    const size_t sm_s = ks > 1 ? std::max(sm, (size_t)split_smem_units(MU) * sizeof(double2)) : sm;
     const int64_t len = n * b;
     int grid_r, grid_b, grid_s, egrid;
     SegView sv{};
@@ -1049,7 +1106,13 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
         grid_r = grid_for(n, mp);
         grid_b = grid_for(nb, mp);
         // S products walk block rows when S is stored as 4x4 blocks
-        grid_s = SF != S_CSR ? grid_for(M->S->bsr_nb, mp) : grid_r;
+        if constexpr (SF != S_CSR) {
+            const int64_t spc = mp.gpc / ks;  // block rows per CTA and pass
+            grid_s = (int)std::max<int64_t>(1, std::min<int64_t>((M->S->bsr_nb + spc - 1) / spc,
+                                                                 (int64_t)sm_count() * 8));
+        } else {
+            grid_s = grid_r;
+        }
         egrid = (int)std::min<int64_t>((len + 255) / 256, (int64_t)sm_count() * 16);
         if (M->red.ensure(std::max(grid_r, std::max(grid_b, grid_s)), (int)b)) return KMSD_ECUDA;
         tk = M->red.tick();
@@ -1101,7 +1164,7 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
         KMSD_CUDA(cudaGraphConditionalHandleCreate(&lp.check, body, 0, cudaGraphCondAssignDefault));
         cudaStream_t bs = M->loop_stream, cs2 = M->check_stream;
         KMSD_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        pcg_spmv_kernel<MU, SF, SEG><<<grid_s, kThreads, sm, bs>>>(S, SB, p, sp, n, mp, c, part, tk, sv, lp);
+        pcg_spmv_kernel<MU, SF, SEG><<<grid_s, kThreads, sm_s, bs>>>(S, SB, p, sp, n, mp, c, part, tk, sv, lp, ks);
         pcg_update_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, bs>>>(y, r, z, p, sp, P, nb, mp, c, 0, M->interval,
                                                                        M->adaptive, part, tk, sv, lp);
         cudaError_t le = cudaGetLastError();
@@ -1123,8 +1186,8 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
             ae = cudaStreamBeginCaptureToGraph(cs2, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                                cudaStreamCaptureModeThreadLocal);
         if (ae == cudaSuccess) {
-            pcg_true_residual_kernel<MU, SF, SEG><<<grid_s, kThreads, sm, cs2>>>(
-                S, SB, q, y, r, t, n, mp, c, M->adaptive, M->gap_ratio, part, tk, cnt, sv, lp);
+            pcg_true_residual_kernel<MU, SF, SEG><<<grid_s, kThreads, sm_s, cs2>>>(
+                S, SB, q, y, r, t, n, mp, c, M->adaptive, M->gap_ratio, part, tk, cnt, sv, lp, ks);
             pcg_restart_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, cs2>>>(r, z, t, P, nb, mp, c, part, tk, sv, lp);
             if (le == cudaSuccess) le = cudaGetLastError();
             cudaGraph_t ib = nullptr;
@@ -1143,14 +1206,15 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
         int slot = 0, pending = 0;
         for (int k = 0; k < maxiter; ++k) {
             const int refresh = ((k + 1) % M->interval) == 0;
-            pcg_spmv_kernel<MU, SF, SEG><<<grid_s, kThreads, sm, s>>>(S, SB, p, sp, n, mp, c, part, tk, sv, Loop{});
+            pcg_spmv_kernel<MU, SF, SEG><<<grid_s, kThreads, sm_s, s>>>(S, SB, p, sp, n, mp, c, part, tk, sv, Loop{},
+                                                                          ks);
             count_launch();
             pcg_update_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, s>>>(y, r, z, p, sp, P, nb, mp, c, refresh, 0,
                                                                           M->adaptive, part, tk, sv, Loop{});
             count_launch();
             if (refresh || M->adaptive) {
-                pcg_true_residual_kernel<MU, SF, SEG><<<grid_s, kThreads, sm, s>>>(
-                    S, SB, q, y, r, t, n, mp, c, M->adaptive, M->gap_ratio, part, tk, cnt, sv, Loop{});
+                pcg_true_residual_kernel<MU, SF, SEG><<<grid_s, kThreads, sm_s, s>>>(
+                    S, SB, q, y, r, t, n, mp, c, M->adaptive, M->gap_ratio, part, tk, cnt, sv, Loop{}, ks);
                 count_launch();
                 pcg_restart_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, s>>>(r, z, t, P, nb, mp, c, part, tk, sv,
                                                                                Loop{});
@@ -1172,7 +1236,7 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
         }
     }
     KMSD_CUDA(cudaGetLastError());
-    pcg_final_kernel<MU, SF, SEG><<<grid_s, kThreads, sm, s>>>(S, SB, q, y, n, mp, c, part, tk, cnt, sv);
+    pcg_final_kernel<MU, SF, SEG><<<grid_s, kThreads, sm_s, s>>>(S, SB, q, y, n, mp, c, part, tk, cnt, sv, ks);
     count_launch();
     pcg_out_kernel<MU, SEG><<<grid_r, kThreads, sm, s>>>(y, Y, n, mp, c, part, tk, cnt, status, fr, sv);
     count_launch();
