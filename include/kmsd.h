@@ -171,6 +171,14 @@ int kmsd_metric_solve(kmsd_metric m, const void *b_in, void *y_out, int64_t b,
  * reference, which solves one system per metric. */
 int kmsd_metric_set_segments(kmsd_metric m, int64_t nseg, const int64_t *row_offsets);
 
+/* Storage of the CG work vectors (r, z, p, S p and the true residual):
+ * KMSD_FP64 (default) or KMSD_MIXED (complex64).  Every operation on them
+ * stays FP64, and so do the right-hand side, the solution, every inner
+ * product and norm, the breakdown test and the true-residual acceptance; the
+ * mixed form halves the solve's vector traffic.  No counterpart in the
+ * reference, whose solve is complex128 throughout. */
+int kmsd_metric_set_storage(kmsd_metric m, int precision);
+
 /* out = D^-1/2 p(W) xi with W = (D^-1/2 S D^-1/2 - center)/half and p the
  * Chebyshev series `coeff` (Clenshaw).  Replaces Metric::sample
  * (cpp/native.cpp:453-479). */

@@ -56,6 +56,7 @@ SIGNATURES = {
     "kmsd_metric_destroy": (None, [P]),
     "kmsd_metric_set_residual_policy": (C.c_int, [P, C.c_int, C.c_int, D]),
     "kmsd_metric_set_segments": (C.c_int, [P, I64, PI64]),
+    "kmsd_metric_set_storage": (C.c_int, [P, C.c_int]),
     "kmsd_metric_solve": (C.c_int, [P, P, P, I64, D, D, C.c_int, C.POINTER(SolveReport), P]),
     "kmsd_metric_sample": (C.c_int, [P, P, P, I64, PD, I64, D, D, P]),
     "kmsd_metric_stats_get": (C.c_int, [P, C.POINTER(MetricStats)]),

@@ -25,18 +25,22 @@ class B200Batch:
     Chebyshev step over all instances, replayed from a CUDA graph.
     Nonorthogonal instances (`overlaps` = one S per instance, `blocks` = the
     block-Jacobi factors (a, b, L) of each instance in its own row numbering,
-    or None for the diagonal preconditioner): FP64, direct moments
-    mu_k = Re<S B, T_k> per instance, S^-1 applied by one segmented PCG per
-    step over all instances (one CG per instance and column, as the reference
-    solves each instance).
+    or None for the diagonal preconditioner): direct moments
+    mu_k = Re<S B, T_k> per instance with an FP64 recurrence, S^-1 applied by
+    one segmented PCG per step over all instances (one CG per instance and
+    column, as the reference solves each instance); precision="mixed" stores
+    the CG work vectors in complex64.
     """
 
     def __init__(self, hamiltonians, precision="mixed", tile_rows=0, overlaps=None, blocks=None, rtol=1e-10,
                  atol=0., maxiter=1000, residual_policy="fixed", check_interval=32, gap_ratio=.1):
         self.lib = _abi.require_library()
         torch = _torch()
-        if overlaps is not None and precision != "fp64":
-            raise ValueError("a batch of nonorthogonal instances runs in FP64 (precision='fp64')")
+        # nonorthogonal instances: FP64 recurrence; precision="mixed" keeps
+        # the CG work vectors of the segmented solve in complex64
+        self.metric_storage = precision if overlaps is not None else None
+        if overlaps is not None:
+            precision = "fp64"
         self.parts = [DeviceCSR(H, self.lib) for H in hamiltonians]
         self.ninst = len(self.parts)
         handles = (C.c_void_p * self.ninst)(*[p.handle.value for p in self.parts])
@@ -72,6 +76,7 @@ class B200Batch:
                               metric_gap_ratio=gap)
         self.hglobal = DeviceCSR(Hg, self.lib)
         self.metric = B200Metric(Sg, Sg.diagonal().real.copy(), gblocks, cfg)
+        self.metric.set_storage(self.metric_storage)
         _check(self.lib, self.lib.kmsd_batch_attach_metric(self.handle, self.hglobal.handle, self.metric.handle,
                                                            float(rtol), float(atol), int(maxiter)))
 

@@ -64,6 +64,31 @@ __device__ __forceinline__ void st(float4 *p, const Pk<float> &a) {
     *p = make_float4(a.re[0], a.im[0], a.re[1], a.im[1]);
 }
 
+// ------------------------------------------------------- CG work-vector storage
+// The work vectors of the metric solve (r, z, p, S p, t) are stored as
+// complex128 or, in the mixed form, complex64; every operation on them is
+// FP64.  stored<W>(v) is v as it reads back after stw into W.
+__device__ __forceinline__ double2 ldw(const double2 *p) { return *p; }
+__device__ __forceinline__ double2 ldw(const float2 *p) {
+    const float2 v = *p;
+    return make_double2(v.x, v.y);
+}
+__device__ __forceinline__ void stw(double2 *p, double2 v) { *p = v; }
+__device__ __forceinline__ void stw(float2 *p, double2 v) { *p = make_float2((float)v.x, (float)v.y); }
+template <class W> __device__ __forceinline__ double2 stored(double2 v) {
+    if constexpr (sizeof(W) == sizeof(float2)) return make_double2((double)(float)v.x, (double)(float)v.y);
+    else return v;
+}
+// Read-only gathers of either storage into FP64 registers.
+__device__ __forceinline__ Pk<double> ldg_d(const double2 *p) { return ldg(p); }
+__device__ __forceinline__ Pk<double> ldg_d(const float2 *p) {
+    const float2 v = __ldg(p);
+    Pk<double> r;
+    r.re[0] = v.x;
+    r.im[0] = v.y;
+    return r;
+}
+
 template <class T> __device__ __forceinline__ Pk<T> pk_zero() {
     Pk<T> r;
 #pragma unroll

@@ -125,6 +125,7 @@ struct kmsd_metric_s {
     double2 *factors = nullptr;
     int maxb = 1;
     int ub = 0;               // uniform block size (block i = rows [i*ub, (i+1)*ub)), else 0
+    int store32 = 0;          // CG work vectors stored as complex64 (the mixed form)
     bool identity = false;
     int adaptive = 0, interval = 32;
     double gap_ratio = .1;

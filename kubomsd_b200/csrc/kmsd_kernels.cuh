@@ -61,6 +61,27 @@ __device__ __forceinline__ void gather_row(const CsrView<T> &A, const typename U
     }
 }
 
+// gather_row for a complex128 matrix over complex128 or complex64 X, with
+// FP64 accumulation (the S products of the metric solve).
+template <int MU, class XV>
+__device__ __forceinline__ void gather_row_d(const CsrView<double> &A, const XV *X, int64_t row, int U, int G,
+                                             int lane, Pk<double> (&acc)[MU]) {
+    const int k0 = __ldg(A.ptr + row), k1 = __ldg(A.ptr + row + 1);
+    for (int k = k0; k < k1; ++k) {
+        const int col = __ldg(A.idx + k);
+        const double vr = __ldg(A.re + k), vi = A.im ? __ldg(A.im + k) : 0.;
+        const XV *src = X + (size_t)col * U;
+#pragma unroll
+        for (int m = 0; m < MU; ++m) {
+            const int u = lane + m * G;
+            if (u < U) {
+                if (A.im) cmac_cplx(acc[m], vr, vi, ldg_d(src + u));
+                else cmac_real(acc[m], vr, ldg_d(src + u));
+            }
+        }
+    }
+}
+
 // Four matrix values starting at a 16-byte aligned element.
 __device__ __forceinline__ void ld4(const float *p, float (&v)[4]) {
     const float4 q = __ldg(reinterpret_cast<const float4 *>(p));
@@ -111,8 +132,8 @@ __device__ __forceinline__ void gather_row_ell(const EllView<T> &A, const typena
 // values are loaded one block row at a time.
 // With ks > 1 this call takes only the blocks part, part + ks, ... of the
 // block row (a split of one block row over ks row groups).
-template <int MU, bool CPLX>
-__device__ __forceinline__ void gather_block_row(const BsrView<double> &A, const double2 *X, int64_t I, int U,
+template <int MU, bool CPLX, class XV = double2>
+__device__ __forceinline__ void gather_block_row(const BsrView<double> &A, const XV *X, int64_t I, int U,
                                                  int G, int lane, Pk<double> (&acc)[4][MU], int part = 0,
                                                  int ks = 1) {
     const int k0 = __ldg(A.bptr + I) + part, k1 = __ldg(A.bptr + I + 1);
@@ -127,7 +148,7 @@ __device__ __forceinline__ void gather_block_row(const BsrView<double> &A, const
         for (int m = 0; m < MU; ++m) {
             const int u = lane + m * G;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) x[m][j] = u < U ? ldg(X + (size_t)(4 * J + j) * U + u) : pk_zero<double>();
+            for (int j = 0; j < 4; ++j) x[m][j] = u < U ? ldg_d(X + (size_t)(4 * J + j) * U + u) : pk_zero<double>();
         }
         const double2 *pr = reinterpret_cast<const double2 *>(A.re + (size_t)k * 16);
 #pragma unroll

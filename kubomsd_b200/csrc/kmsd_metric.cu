@@ -17,6 +17,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <utility>
 
 #include "kmsd.h"
@@ -280,9 +281,9 @@ __global__ void __launch_bounds__(256) pcg_scale_kernel(const double2 *B, int64_
 }
 
 // ---- init: q = B/safe, r = q, y = 0, z = M^-1 r; sums |q|^2 and Re<r,z>
-template <int MU, int MAXB, bool SEG>
+template <int MU, int MAXB, bool SEG, class W>
 __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
-    pcg_init_kernel(const double2 *B, double2 *q, double2 *y, double2 *r, double2 *z, Pre P, int64_t nb, RowMap mp,
+    pcg_init_kernel(const double2 *B, double2 *q, double2 *y, W *r, W *z, Pre P, int64_t nb, RowMap mp,
                     ColPtr c, double rtol, double atol, double2 *partial, Ticket *tk, SegView sv) {
     extern __shared__ double2 smem[];
     const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
@@ -308,9 +309,9 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
                     const double2 v = B[o];
                     const double2 qq = make_double2(v.x / sf, v.y / sf);
                     q[o] = qq;
-                    r[o] = qq;
+                    stw(r + o, qq);
                     y[o] = make_double2(0., 0.);
-                    rr[i] = qq;
+                    rr[i] = stored<W>(qq);
                     acc[mm][0].x += qq.x * qq.x + qq.y * qq.y;
                 }
             }
@@ -318,8 +319,9 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
 #pragma unroll
             for (int i = 0; i < MAXB; ++i) {
                 if (i < m) {
-                    z[(size_t)(r0 + i) * U + u] = zz[i];
-                    acc[mm][0].y += rr[i].x * zz[i].x + rr[i].y * zz[i].y;
+                    stw(z + (size_t)(r0 + i) * U + u, zz[i]);
+                    const double2 zs = stored<W>(zz[i]);
+                    acc[mm][0].y += rr[i].x * zs.x + rr[i].y * zs.y;
                 }
             }
         }
@@ -363,14 +365,14 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
 }
 
 // p = active ? z : 0
-template <bool SEG>
-__global__ void pcg_pinit_kernel(const double2 *z, double2 *p, int64_t len, RowMap mp, ColPtr c, SegView sv) {
+template <bool SEG, class W>
+__global__ void pcg_pinit_kernel(const W *z, W *p, int64_t len, RowMap mp, ColPtr c, SegView sv) {
     if constexpr (!SEG) {
         const int U = mp.U;
         for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len;
              i += (int64_t)gridDim.x * blockDim.x) {
             const int j = (int)(i % U);
-            p[i] = c.active[j] ? z[i] : make_double2(0., 0.);
+            p[i] = c.active[j] ? z[i] : W{};
         }
     } else {
         const int g = threadIdx.x / mp.G, lane = threadIdx.x % mp.G;
@@ -378,7 +380,7 @@ __global__ void pcg_pinit_kernel(const double2 *z, double2 *p, int64_t len, RowM
         for (int64_t row = x.r0 + (int64_t)x.lc * mp.gpc + g; row < x.r1; row += (int64_t)x.nct * mp.gpc)
             for (int u = lane; u < mp.U; u += mp.G) {
                 const size_t o = (size_t)row * mp.U + u;
-                p[o] = c.active[(size_t)x.s * mp.U + u] ? z[o] : make_double2(0., 0.);
+                p[o] = c.active[(size_t)x.s * mp.U + u] ? z[o] : W{};
             }
     }
 }
@@ -399,8 +401,8 @@ enum { S_CSR = 0, S_BSR_REAL = 1, S_BSR_CPLX = 2 };
 // memory then holds split_smem_units(MU) double2.
 __host__ __device__ constexpr int split_smem_units(int mu) { return 1024 * mu; }
 
-template <int MU, int SF, class F>
-__device__ __forceinline__ void for_rows_spmv(const CsrView<double> &S, const BsrView<double> &SB, const double2 *X,
+template <int MU, int SF, class XV, class F>
+__device__ __forceinline__ void for_rows_spmv(const CsrView<double> &S, const BsrView<double> &SB, const XV *X,
                                               const Ctx &x, const RowMap &mp, int g, int lane, int ks, F &&f) {
     if (SF != S_CSR && ks > 1) {
         extern __shared__ double2 part_sums[];  // [group][4 rows][MU][G lanes]
@@ -456,7 +458,8 @@ __device__ __forceinline__ void for_rows_spmv(const CsrView<double> &S, const Bs
             Pk<double> yv[MU];
 #pragma unroll
             for (int m = 0; m < MU; ++m) yv[m] = pk_zero<double>();
-            gather_row<double, MU>(S, X, row, mp.U, mp.G, lane, yv);
+            if constexpr (std::is_same<XV, double2>::value) gather_row<double, MU>(S, X, row, mp.U, mp.G, lane, yv);
+            else gather_row_d<MU>(S, X, row, mp.U, mp.G, lane, yv);
             f(row, yv);
         }
     }
@@ -482,9 +485,9 @@ __device__ __forceinline__ void loop_count(const Loop &lp) {
 }
 
 // ---- sp = S p, curvature <p, sp>, alpha, breakdown
-template <int MU, int SF, bool SEG>
+template <int MU, int SF, bool SEG, class W>
 __global__ void __launch_bounds__(256)
-    pcg_spmv_kernel(CsrView<double> S, BsrView<double> SB, const double2 *p, double2 *sp, int64_t n, RowMap mp,
+    pcg_spmv_kernel(CsrView<double> S, BsrView<double> SB, const W *p, W *sp, int64_t n, RowMap mp,
                     ColPtr c, double2 *partial, Ticket *tk, SegView sv, Loop lp, int ks) {
     loop_count(lp);
     if (*(volatile int *)c.flags) return;
@@ -499,8 +502,9 @@ __global__ void __launch_bounds__(256)
             const int u = lane + m * mp.G;
             if (u < mp.U) {
                 const size_t o = (size_t)row * mp.U + u;
-                sp[o] = make_double2(yv[m].re[0], yv[m].im[0]);
-                const double2 xv = p[o];
+                // <p, S p> from the stored p and the exact FP64 product
+                stw(sp + o, make_double2(yv[m].re[0], yv[m].im[0]));
+                const double2 xv = ldw(p + o);
                 acc[m][0].x += xv.x * yv[m].re[0] + xv.y * yv[m].im[0];
                 acc[m][0].y += xv.x * yv[m].im[0] - xv.y * yv[m].re[0];
             }
@@ -539,9 +543,9 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---- y += alpha p, r -= alpha sp, z = M^-1 r; sums |r|^2, Re<r,z>
-template <int MU, int MAXB, bool SEG>
+template <int MU, int MAXB, bool SEG, class W>
 __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
-    pcg_update_kernel(double2 *y, double2 *r, double2 *z, const double2 *p, const double2 *sp, Pre P, int64_t nb,
+    pcg_update_kernel(double2 *y, W *r, W *z, const W *p, const W *sp, Pre P, int64_t nb,
                       RowMap mp, ColPtr c, int refresh, int interval, int adaptive, double2 *partial, Ticket *tk,
                       SegView sv, Loop lp) {
     loop_count(lp);
@@ -570,24 +574,25 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
             for (int i = 0; i < MAXB; ++i) {
                 if (i < m) {
                     const size_t o = (size_t)(r0 + i) * U + u;
-                    const double2 pv = p[o], sv2 = sp[o];
-                    double2 yv = y[o], rv = r[o];
+                    const double2 pv = ldw(p + o), sv2 = ldw(sp + o);
+                    double2 yv = y[o], rv = ldw(r + o);
                     yv.x += pv.x * al;
                     yv.y += pv.y * al;
                     rv.x -= sv2.x * al;
                     rv.y -= sv2.y * al;
                     y[o] = yv;
-                    r[o] = rv;
-                    rr[i] = rv;
-                    acc[mm][0].x += rv.x * rv.x + rv.y * rv.y;
+                    stw(r + o, rv);
+                    rr[i] = stored<W>(rv);
+                    acc[mm][0].x += rr[i].x * rr[i].x + rr[i].y * rr[i].y;
                 }
             }
             precond<MAXB>(P, bi, r0, m, rr, zz);
 #pragma unroll
             for (int i = 0; i < MAXB; ++i) {
                 if (i < m) {
-                    z[(size_t)(r0 + i) * U + u] = zz[i];
-                    acc[mm][0].y += rr[i].x * zz[i].x + rr[i].y * zz[i].y;
+                    stw(z + (size_t)(r0 + i) * U + u, zz[i]);
+                    const double2 zs = stored<W>(zz[i]);
+                    acc[mm][0].y += rr[i].x * zs.x + rr[i].y * zs.y;
                 }
             }
         }
@@ -610,7 +615,12 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
         const bool candidate = __syncthreads_or(cand);
         // in a device-driven loop the iteration index lives in flags[5]
         if (interval > 0) refresh = ((*(volatile int *)(c.flags + 5) + 1) % interval) == 0;
-        const bool check = refresh || (adaptive && candidate);
+        // Mixed form: the recursive residual of complex64 work vectors can sit
+        // below the threshold while the true residual does not, so a column
+        // that reaches it is checked in FP64 (as the adaptive policy does)
+        // before it stops, and restarted from its true residual otherwise.
+        constexpr bool kMixed = sizeof(W) == sizeof(float2);
+        const bool check = refresh || ((adaptive || kMixed) && candidate);
         bool act_now = false;
         if (j < U) {
             if (!check) {
@@ -657,10 +667,10 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
 }
 
 // ---- true residual t = q - S y; sums |t|^2 and |t - r|^2; refresh decision
-template <int MU, int SF, bool SEG>
+template <int MU, int SF, bool SEG, class W>
 __global__ void __launch_bounds__(256)
     pcg_true_residual_kernel(CsrView<double> S, BsrView<double> SB, const double2 *q, const double2 *y,
-                             const double2 *r, double2 *t, int64_t n, RowMap mp, ColPtr c, int adaptive,
+                             const W *r, W *t, int64_t n, RowMap mp, ColPtr c, int adaptive,
                              double gap_ratio, double2 *partial, Ticket *tk, Counters *cnt, SegView sv, Loop lp,
                              int ks) {
     loop_count(lp);
@@ -679,9 +689,9 @@ __global__ void __launch_bounds__(256)
                 const int u = lane + m * mp.G;
                 if (u < mp.U) {
                     const size_t o = (size_t)row * mp.U + u;
-                    const double2 qv = q[o], rv = r[o];
+                    const double2 qv = q[o], rv = ldw(r + o);
                     const double2 tv = make_double2(qv.x - sy[m].re[0], qv.y - sy[m].im[0]);
-                    t[o] = tv;
+                    stw(t + o, tv);
                     acc[m][0].x += tv.x * tv.x + tv.y * tv.y;
                     const double dx = tv.x - rv.x, dy = tv.y - rv.y;
                     acc[m][0].y += dx * dx + dy * dy;
@@ -728,9 +738,9 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---- after a check: r <- t on restarted columns, z = M^-1 r, beta
-template <int MU, int MAXB, bool SEG>
+template <int MU, int MAXB, bool SEG, class W>
 __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
-    pcg_restart_kernel(double2 *r, double2 *z, const double2 *t, Pre P, int64_t nb, RowMap mp, ColPtr c,
+    pcg_restart_kernel(W *r, W *z, const W *t, Pre P, int64_t nb, RowMap mp, ColPtr c,
                        double2 *partial, Ticket *tk, SegView sv, Loop lp) {
     loop_count(lp);
     if (*(volatile int *)c.flags || !*(volatile int *)(c.flags + 1)) return;
@@ -756,10 +766,10 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
             for (int i = 0; i < MAXB; ++i) {
                 if (i < m) {
                     const size_t o = (size_t)(r0 + i) * U + u;
-                    double2 rv = r[o];
+                    double2 rv = ldw(r + o);
                     if (rs) {
-                        rv = t[o];
-                        r[o] = rv;
+                        rv = ldw(t + o);
+                        stw(r + o, rv);
                     }
                     rr[i] = rv;
                 }
@@ -768,8 +778,9 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
 #pragma unroll
             for (int i = 0; i < MAXB; ++i) {
                 if (i < m) {
-                    z[(size_t)(r0 + i) * U + u] = zz[i];
-                    acc[mm][0].y += rr[i].x * zz[i].x + rr[i].y * zz[i].y;
+                    stw(z + (size_t)(r0 + i) * U + u, zz[i]);
+                    const double2 zs = stored<W>(zz[i]);
+                    acc[mm][0].y += rr[i].x * zs.x + rr[i].y * zs.y;
                 }
             }
         }
@@ -811,8 +822,8 @@ __device__ __forceinline__ double2 direction(const ColPtr &c, size_t cj, double2
     const double be = c.beta[cj];
     return make_double2(zv.x + pv.x * be, zv.y + pv.y * be);
 }
-template <bool SEG>
-__global__ void pcg_direction_kernel(const double2 *z, double2 *p, int64_t len, RowMap mp, ColPtr c, SegView sv,
+template <bool SEG, class W>
+__global__ void pcg_direction_kernel(const W *z, W *p, int64_t len, RowMap mp, ColPtr c, SegView sv,
                                      Loop lp) {
     loop_count(lp);
     if (*(volatile int *)c.flags) return;
@@ -822,10 +833,10 @@ __global__ void pcg_direction_kernel(const double2 *z, double2 *p, int64_t len, 
              i += (int64_t)gridDim.x * blockDim.x) {
             const int j = (int)(i % U);
             if (!c.active[j]) {
-                p[i] = make_double2(0., 0.);
+                stw(p + i, make_double2(0., 0.));
             } else {
-                const double2 zv = z[i];
-                p[i] = c.restart[j] ? zv : direction(c, j, zv, p[i]);
+                const double2 zv = ldw(z + i);
+                stw(p + i, c.restart[j] ? zv : direction(c, j, zv, ldw(p + i)));
             }
         }
     } else {
@@ -834,7 +845,7 @@ __global__ void pcg_direction_kernel(const double2 *z, double2 *p, int64_t len, 
         for (int64_t row = x.r0 + (int64_t)x.lc * mp.gpc + g; row < x.r1; row += (int64_t)x.nct * mp.gpc)
             for (int u = lane; u < mp.U; u += mp.G) {
                 const size_t o = (size_t)row * mp.U + u;
-                p[o] = direction(c, (size_t)x.s * mp.U + u, z[o], p[o]);
+                stw(p + o, direction(c, (size_t)x.s * mp.U + u, ldw(z + o), ldw(p + o)));
             }
     }
 }
@@ -1072,7 +1083,7 @@ namespace {
 // nothing), or from the device as the WHILE node of a capturing stream.
 enum { kHostLoop = 0, kPrepare = 1, kDeviceLoop = 2 };
 
-template <int MU, int MAXB, int SF, bool SEG>
+template <int MU, int MAXB, int SF, bool SEG, class W>
 int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rtol, double atol, int maxiter,
             cudaStream_t s, int *status, FailReportFull *fr, int *claimed, int mode) {
     const int64_t n = M->n;
@@ -1123,8 +1134,8 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
     Pre P{M->diag, M->bstart, M->foff, M->factors, M->ub};
     const CsrView<double> S = M->S->view64();
     Counters *cnt = M->dcount.as<Counters>();
-    double2 *q = M->q.as<double2>(), *y = M->y.as<double2>(), *r = M->r.as<double2>(), *z = M->z.as<double2>(),
-            *p = M->p.as<double2>(), *sp = M->sp.as<double2>(), *t = M->t.as<double2>();
+    double2 *q = M->q.as<double2>(), *y = M->y.as<double2>();
+    W *r = M->r.as<W>(), *z = M->z.as<W>(), *p = M->p.as<W>(), *sp = M->sp.as<W>(), *t = M->t.as<W>();
     double2 *part = M->red.part();
 
     KMSD_CUDA(cudaMemsetAsync(c.flags, 0, 8 * sizeof(int), s));
@@ -1212,7 +1223,7 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
             pcg_update_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, s>>>(y, r, z, p, sp, P, nb, mp, c, refresh, 0,
                                                                           M->adaptive, part, tk, sv, Loop{});
             count_launch();
-            if (refresh || M->adaptive) {
+            if (refresh || M->adaptive || M->store32) {
                 pcg_true_residual_kernel<MU, SF, SEG><<<grid_s, kThreads, sm_s, s>>>(
                     S, SB, q, y, r, t, n, mp, c, M->adaptive, M->gap_ratio, part, tk, cnt, sv, Loop{}, ks);
                 count_launch();
@@ -1251,31 +1262,35 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
 using PcgFn = int (*)(kmsd_metric_s *, const double2 *, double2 *, int64_t, double, double, int, cudaStream_t,
                       int *, FailReportFull *, int *, int);
 
-template <int MAXB, int SF, bool SEG>
+template <int MAXB, int SF, bool SEG, class W>
 PcgFn pick_mu(int mu) {
     switch (mu) {
-        case 1: return run_pcg<1, MAXB, SF, SEG>;
-        case 2: return run_pcg<2, MAXB, SF, SEG>;
+        case 1: return run_pcg<1, MAXB, SF, SEG, W>;
+        case 2: return run_pcg<2, MAXB, SF, SEG, W>;
     }
     return nullptr;
 }
-template <int SF, bool SEG>
+template <int SF, bool SEG, class W>
 PcgFn pick_b(int mu, int maxb) {
-    if (maxb <= 1) return pick_mu<1, SF, SEG>(mu);
-    if (maxb <= 4) return pick_mu<4, SF, SEG>(mu);
-    if (maxb <= 8) return pick_mu<8, SF, SEG>(mu);
-    if (maxb <= 32) return pick_mu<32, SF, SEG>(mu);
+    if (maxb <= 1) return pick_mu<1, SF, SEG, W>(mu);
+    if (maxb <= 4) return pick_mu<4, SF, SEG, W>(mu);
+    if (maxb <= 8) return pick_mu<8, SF, SEG, W>(mu);
+    if (maxb <= 32) return pick_mu<32, SF, SEG, W>(mu);
     return nullptr;
 }
-template <bool SEG>
+template <bool SEG, class W>
 PcgFn pick_s(int mu, int maxb, int sf) {
     switch (sf) {
-        case S_BSR_REAL: return pick_b<S_BSR_REAL, SEG>(mu, maxb);
-        case S_BSR_CPLX: return pick_b<S_BSR_CPLX, SEG>(mu, maxb);
+        case S_BSR_REAL: return pick_b<S_BSR_REAL, SEG, W>(mu, maxb);
+        case S_BSR_CPLX: return pick_b<S_BSR_CPLX, SEG, W>(mu, maxb);
     }
-    return pick_b<S_CSR, SEG>(mu, maxb);
+    return pick_b<S_CSR, SEG, W>(mu, maxb);
 }
-PcgFn pick(int mu, int maxb, int sf, bool seg) { return seg ? pick_s<true>(mu, maxb, sf) : pick_s<false>(mu, maxb, sf); }
+// store32: the CG work vectors in complex64 (the mixed form)
+PcgFn pick(int mu, int maxb, int sf, bool seg, bool store32) {
+    if (store32) return seg ? pick_s<true, float2>(mu, maxb, sf) : pick_s<false, float2>(mu, maxb, sf);
+    return seg ? pick_s<true, double2>(mu, maxb, sf) : pick_s<false, double2>(mu, maxb, sf);
+}
 
 }  // namespace
 
@@ -1292,7 +1307,7 @@ int kmsd_metric_s::solve(const double2 *B, double2 *Y, int64_t b, double rtol, d
     // 4x4 block rows may not straddle two segments
     const bool bsr = S->bsr_nb > 0 && (!seg || seg_aligned4);
     const int sf = bsr ? (S->bsr64().im ? S_BSR_CPLX : S_BSR_REAL) : S_CSR;
-    PcgFn fn = pick(mu_for(mp), nblocks ? maxb : 1, sf, seg);
+    PcgFn fn = pick(mu_for(mp), nblocks ? maxb : 1, sf, seg, store32 != 0);
     if (!fn) return fail(KMSD_EINVAL, "unsupported metric block size / column count");
     const bool sync = status == nullptr;
     // Synchronous calls use a private status word and report.
@@ -1370,7 +1385,7 @@ int kmsd_metric_s::prepare_dev(int64_t b) {
     const RowMap mp = make_map((int)b, kThreads);
     const bool bsr = S->bsr_nb > 0 && (!seg || seg_aligned4);
     const int sf = bsr ? (S->bsr64().im ? S_BSR_CPLX : S_BSR_REAL) : S_CSR;
-    PcgFn fn = pick(mu_for(mp), nblocks ? maxb : 1, sf, seg);
+    PcgFn fn = pick(mu_for(mp), nblocks ? maxb : 1, sf, seg, store32 != 0);
     if (!fn) return fail(KMSD_EINVAL, "unsupported metric block size / column count");
     if (!loop_stream) KMSD_CUDA(cudaStreamCreateWithFlags(&loop_stream, cudaStreamNonBlocking));
     if (!check_stream) KMSD_CUDA(cudaStreamCreateWithFlags(&check_stream, cudaStreamNonBlocking));
@@ -1389,7 +1404,7 @@ int kmsd_metric_s::solve_dev(const double2 *B, double2 *Y, int64_t b, double rto
     const RowMap mp = make_map((int)b, kThreads);
     const bool bsr = S->bsr_nb > 0 && (!seg || seg_aligned4);
     const int sf = bsr ? (S->bsr64().im ? S_BSR_CPLX : S_BSR_REAL) : S_CSR;
-    PcgFn fn = pick(mu_for(mp), nblocks ? maxb : 1, sf, seg);
+    PcgFn fn = pick(mu_for(mp), nblocks ? maxb : 1, sf, seg, store32 != 0);
     if (!fn) return fail(KMSD_EINVAL, "unsupported metric block size / column count");
     if (!loop_stream) KMSD_CUDA(cudaStreamCreateWithFlags(&loop_stream, cudaStreamNonBlocking));
     if (!check_stream) KMSD_CUDA(cudaStreamCreateWithFlags(&check_stream, cudaStreamNonBlocking));
@@ -1422,7 +1437,7 @@ int kmsd_metric_s::solve_dev(const double2 *B, double2 *Y, int64_t b, double rto
     const std::vector<uint64_t> key = {(uint64_t)(uintptr_t)B, (uint64_t)(uintptr_t)Y, (uint64_t)b, bits(rtol),
                                        bits(atol), (uint64_t)maxiter, (uint64_t)(uintptr_t)status,
                                        (uint64_t)(uintptr_t)fail_report, (uint64_t)adaptive, (uint64_t)interval,
-                                       bits(gap_ratio)};
+                                       bits(gap_ratio), (uint64_t)store32};
     auto it = graphs.find(key);
     if (it == graphs.end()) {
         if (graphs.size() >= 32) {  // bounded cache
@@ -1658,6 +1673,12 @@ int kmsd_metric_set_segments(kmsd_metric m, int64_t nseg, const int64_t *row_off
     m->seg_blk0 = blk;
     m->seg_aligned4 = true;
     for (int64_t s = 0; s <= nseg; ++s) m->seg_aligned4 = m->seg_aligned4 && row_offsets[s] % 4 == 0;
+    return KMSD_OK;
+}
+
+int kmsd_metric_set_storage(kmsd_metric m, int precision) {
+    if (!m || (precision != KMSD_FP64 && precision != KMSD_MIXED)) return fail(KMSD_EINVAL, "invalid metric storage");
+    m->store32 = precision == KMSD_MIXED;
     return KMSD_OK;
 }
 

@@ -244,6 +244,8 @@ class B200Metric:
         other.S = self.S
         other.n = self.n
         B200Metric._init_handle(other, diag, blocks, config)
+        if getattr(self, "storage", "fp64") == "mixed":
+            other.set_storage("mixed")
         return other
 
     def _init_handle(self, diag, blocks, config):
@@ -275,6 +277,13 @@ class B200Metric:
         self._set_policy(*self.policy)
         self.identity = bool(self.lib.kmsd_metric_is_identity(handle))
         self.nseg = 1
+
+    def set_storage(self, precision):
+        """Storage of the CG work vectors: "fp64" or "mixed" (complex64; all
+        arithmetic, the solution, inner products and tests stay FP64)."""
+        _check(self.lib, self.lib.kmsd_metric_set_storage(self.handle, _abi.KMSD_MIXED if precision == "mixed"
+                                                          else _abi.KMSD_FP64))
+        self.storage = precision
 
     def set_segments(self, offsets):
         """Declare S block-diagonal over the row ranges offsets[s]:offsets[s+1]
@@ -393,6 +402,12 @@ class B200Operators:
         self.S = metric.S
         self.n = self.H.n
         self.precision = precision or getattr(config, "precision", "fp64")
+        # The mixed form on a nonorthogonal basis: the metric solve keeps its
+        # CG work vectors in complex64 (FP64 arithmetic, solution, inner
+        # products and tests) while the Chebyshev recurrence stays FP64.
+        self.engine_precision = self.precision if metric.identity else "fp64"
+        if self.precision == "mixed" and not metric.identity:
+            metric.set_storage("mixed")
         self.doubling = bool(getattr(config, "moment_doubling", False))
         kinds = (C.c_int * 3)()
         mats = (C.c_void_p * 9)()
@@ -423,7 +438,7 @@ class B200Operators:
         cfg = self._config
         rc = self.lib.kmsd_engine_create(self.H.handle, self.metric.handle, self._kinds, self._mats,
                                          float(cfg.metric_rtol), float(cfg.metric_atol), int(cfg.metric_maxiter),
-                                         HBAR_EV_FS, _abi.KMSD_MIXED if self.precision == "mixed" else _abi.KMSD_FP64,
+                                         HBAR_EV_FS, _abi.KMSD_MIXED if self.engine_precision == "mixed" else _abi.KMSD_FP64,
                                          C.byref(handle))
         _check(self.lib, rc)
         self.handle = handle
@@ -453,7 +468,7 @@ class B200Operators:
         return _diag_dict(arrays, m.value)
 
     def _cols(self):
-        return MAX_COLS_MIXED if self.precision == "mixed" else MAX_COLS
+        return MAX_COLS_MIXED if self.engine_precision == "mixed" else MAX_COLS
 
     # -- operations (same names and signatures as NativeOperators)
     def _h_action(self, B):
@@ -507,7 +522,7 @@ class B200Operators:
             raise ValueError("invalid augmented block columns")
         nb = b // (nd + 1)
         step = max(1, self._cols() // (nd + 1))
-        if self.precision == "mixed" and nd:
+        if self.engine_precision == "mixed" and nd:
             step -= step % 2
         out = torch.empty_like(t)
         for s0 in range(0, nb, step):
