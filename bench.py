@@ -62,6 +62,9 @@ def parse():
                         "(8000 atoms x 4 orbitals, kappa(S)=50, block-Jacobi PCG to 1e-10, R=32, M=1024); "
                         "batch: a ragged batch of 32 nonorthogonal sp3 instances (4,000-32,000 orbitals), R=16; "
                         "serving: a Poisson request stream through the continuous-batching service")
+    p.add_argument("--metric-storage", choices=["fp64", "mixed"], default="fp64",
+                   help="diamond / batch workloads: storage of the CG work vectors (mixed: complex64, FP64 "
+                        "arithmetic, solution, inner products and tests)")
     p.add_argument("--no-compare", action="store_true", help="skip the FP64 / direct comparison lines")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -196,6 +199,7 @@ def run_diamond(args):
                           metric_check_interval=32, metric_gap_ratio=.1, metric_solver="pcg", precision="fp64",
                           moment_doubling=False)
     metric = B200Metric(S, S.diagonal().real.copy(), blocks, cfg)
+    metric.set_storage(args.metric_storage)
     eng = B200Operators(SimpleNamespace(host_H=m.H, metric=SimpleNamespace(native=metric), velocity={},
                                         position={}, composite=m.composite), cfg)
     R, M = 32, args.moments if args.moments != 4096 else 1024
@@ -223,6 +227,7 @@ def run_diamond(args):
                       "data": "synthetic (seeded diamond sp3 model, NumPy PCG64 phases)",
                       "config": {"workload": f"KPM moments, nonorthogonal diamond sp3 {m.n} orbitals, kappa(S)=50, "
                                              f"block-Jacobi PCG rtol 1e-10, R={R}, M={M}",
+                                 "metric_storage": args.metric_storage,
                                  "spectral_bounds_eV": list(bounds), "metric_solves_per_step": calls / args.steps,
                                  "pcg_iterations_per_solve": iters / max(calls, 1)},
                       "gpu_launches": int(lib.kmsd_kernel_launches() - l0),
@@ -254,7 +259,7 @@ def run_batch(args):
     R, M = 16, args.moments if args.moments != 4096 else 64
     c, a = 0., 40.
     phases = [torch.from_numpy(kpm.random_phases(m.n, 20261019 + i, range(R))).cuda() for i, m in enumerate(ms)]
-    bt = B200Batch(Hs, precision="fp64", overlaps=Ss, blocks=blocks, rtol=1e-10)
+    bt = B200Batch(Hs, precision=args.metric_storage, overlaps=Ss, blocks=blocks, rtol=1e-10)
     B = bt.concat(phases)
     N = bt.n
     for _ in range(args.warmup):
@@ -302,6 +307,7 @@ def run_batch(args):
                                              f"({N:,} in total), kappa(S)=50, block-Jacobi PCG rtol 1e-10, R={R}, "
                                              f"M={M}, FP64",
                                  "spectral_bounds_eV": [c - a, c + a], "segmented_solves_per_step": solves,
+                                 "metric_storage": args.metric_storage,
                                  "pcg_iterations_per_solve": iters},
                       "gpu_launches": launches,
                       "separate_calls": {"ms": ms_sep, "value": N * M * R / (ms_sep / 1e3),
