@@ -334,6 +334,17 @@ enum { HSRC_SOLVED = 0, HSRC_CSR = 1, HSRC_ELL = 2, HSRC_ELL4 = 3, HSRC_ELL8 = 4
 // Minimum resident CTAs per SM asked of the compiler for the one-unit-per-lane
 // step kernels.  The kernel is latency bound; on B200 four CTAs of 256
 // threads (<= 64 registers) measured best for the moment steps.
+// Moment steps over a 4- or 8-wide real ELL form take two rows per row group
+// and iteration (all loads of both rows issued before either row is
+// computed), at KMSD_STEP_PAIR_MINB CTAs per SM.  On the 4.19M-site
+// honeycomb moment step this measured 1.5 % faster than one row at four CTAs
+// per SM, and two rows at three CTAs per SM were slower.  0 disables it.
+#ifndef KMSD_STEP_PAIR
+#define KMSD_STEP_PAIR 1
+#endif
+#ifndef KMSD_STEP_PAIR_MINB
+#define KMSD_STEP_PAIR_MINB 2
+#endif
 #ifndef KMSD_STEP_MINB
 #define KMSD_STEP_MINB 4
 #endif
@@ -373,8 +384,14 @@ __device__ __forceinline__ void gather_prefetched(const EllRow<T, PF> &r, const 
     }
 }
 
+template <int MU, int MODE, int HSRC>
+constexpr bool step_pairs() {
+    return KMSD_STEP_PAIR && MU == 1 && MODE == MODE_DOUBLING && (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8);
+}
+
 template <class T, int MU, int MODE, int HSRC, bool INLINE_V>
-__global__ void __launch_bounds__(256, (MU == 1 && MODE != MODE_SERIES ? KMSD_STEP_MINB : 1))
+__global__ void __launch_bounds__(256, (step_pairs<MU, MODE, HSRC>() ? KMSD_STEP_PAIR_MINB
+                                        : MU == 1 && MODE != MODE_SERIES ? KMSD_STEP_MINB : 1))
     cheb_step_kernel(const StepArgs<T> a) {
     using V = typename Unit<T>::vec;
     constexpr int C = Unit<T>::C;
@@ -393,10 +410,56 @@ __global__ void __launch_bounds__(256, (MU == 1 && MODE != MODE_SERIES ? KMSD_ST
     bool bad = false;
     constexpr int PF = HSRC == HSRC_ELL4 ? 1 : HSRC == HSRC_ELL8 ? 2 : 1;
     const int64_t stride = (int64_t)gridDim.x * mp.gpc;
+    if constexpr (step_pairs<MU, MODE, HSRC>()) {
+        // Rows `row` and `row + stride` per iteration; the ELL rows of the
+        // next pair are loaded one iteration ahead.
+        const int u = lane;
+        const int64_t first = (int64_t)blockIdx.x * mp.gpc + g;
+        EllRow<T, PF> aheadA, aheadB;
+        if (first < a.n) ell_row_load<T, PF>(a.E, first, aheadA);
+        if (first + stride < a.n) ell_row_load<T, PF>(a.E, first + stride, aheadB);
+        for (int64_t row = first; row < a.n; row += 2 * stride) {
+            const int64_t rowB = row + stride;
+            const bool hasB = rowB < a.n;
+            const EllRow<T, PF> curA = aheadA, curB = aheadB;
+            if (row + 2 * stride < a.n) ell_row_load<T, PF>(a.E, row + 2 * stride, aheadA);
+            if (rowB + 2 * stride < a.n) ell_row_load<T, PF>(a.E, rowB + 2 * stride, aheadB);
+            if (u >= mp.U) continue;
+            const size_t oA = (size_t)row * mp.U + u, oB = (size_t)rowB * mp.U + u;
+            const Pk<T> xA = ld(a.curr + oA), pA = a.first ? pk_zero<T>() : ld(a.prev + oA);
+            Pk<T> xB = pk_zero<T>(), pB = pk_zero<T>();
+            if (hasB) {
+                xB = ld(a.curr + oB);
+                if (!a.first) pB = ld(a.prev + oB);
+            }
+            Pk<T> hA[1] = {pk_zero<T>()}, hB[1] = {pk_zero<T>()};
+            gather_prefetched<T, 1, PF>(curA, a.curr, mp.U, mp.G, lane, hA);
+            if (hasB) gather_prefetched<T, 1, PF>(curB, a.curr, mp.U, mp.G, lane, hB);
+#pragma unroll
+            for (int r2 = 0; r2 < 2; ++r2) {
+                if (r2 == 1 && !hasB) break;
+                const Pk<T> &x = r2 ? xB : xA;
+                const Pk<T> &pv = r2 ? pB : pA;
+                const Pk<T> &hv = r2 ? hB[0] : hA[0];
+                Pk<T> nx;
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    const T tr = rdiv(hv.re[c] - cen * x.re[c], hal, a.inv_half);
+                    const T ti = rdiv(hv.im[c] - cen * x.im[c], hal, a.inv_half);
+                    nx.re[c] = a.first ? tr : T(2) * tr - pv.re[c];
+                    nx.im[c] = a.first ? ti : T(2) * ti - pv.im[c];
+                    acc0[0][c].x += (double)x.re[c] * (double)x.re[c] + (double)x.im[c] * (double)x.im[c];
+                    acc1[0][c].x += (double)x.re[c] * (double)nx.re[c] + (double)x.im[c] * (double)nx.im[c];
+                }
+                st(a.next + (r2 ? oB : oA), nx);
+            }
+        }
+    }
     EllRow<T, PF> ahead;
-    if ((HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8) && (int64_t)blockIdx.x * mp.gpc + g < a.n)
+    if (!step_pairs<MU, MODE, HSRC>() && (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8) &&
+        (int64_t)blockIdx.x * mp.gpc + g < a.n)
         ell_row_load<T, PF>(a.E, (int64_t)blockIdx.x * mp.gpc + g, ahead);
-    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; row < a.n; row += stride) {
+    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; !step_pairs<MU, MODE, HSRC>() && row < a.n; row += stride) {
         EllRow<T, PF> cur;
         if (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8) {
             cur = ahead;
