@@ -332,7 +332,8 @@ def run_serving(args):
                                 replicas=8),
     }
     duration = float(os.environ.get("KMSD_SERVING_SECONDS", "30"))
-    reqs = poisson_stream(20., duration, models, seed=5)
+    rate = float(os.environ.get("KMSD_SERVING_RATE", "20"))
+    reqs = poisson_stream(rate, duration, models, seed=5)
     srv = Server(models, slots=8, hbm_budget_bytes=150 * 10 ** 9)
     t0 = time.perf_counter()
     res = srv.serve(reqs)
@@ -344,9 +345,10 @@ def run_serving(args):
                       "warmup": 0, "ms_per_step": wall / max(len(res), 1) * 1e3, "higher_is_better": True,
                       "scaling": "weak", "vs_baseline": None, "dtype": "c64 vectors / f64 accumulation (lattices), "
                       "c128 (sp3)", "data": "synthetic Poisson stream (seed 5)",
-                      "config": {"workload": f"serving: Poisson 20 req/s for {duration:g} s, M in {{512,1024,2048}}, "
-                                             "R in {8,32}, models 16k-4.2M sites / 8k sp3 orbitals, 8 slots, "
-                                             "HBM budget 150 GB"},
+                      "config": {"workload": f"serving: Poisson {rate:g} req/s for {duration:g} s, M in "
+                                             "{512,1024,2048}, R in {8,32}, models "
+                                             + ", ".join(f"{k} ({m.n:,} orbitals)" for k, m in models.items())
+                                             + ", 8 slots, HBM budget 150 GB"},
                       "latency": summ, "errors": len(srv.errors), "offered_requests": len(reqs),
                       "wall_s": wall}))
 
