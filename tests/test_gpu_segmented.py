@@ -142,3 +142,24 @@ def test_nonorthogonal_batch_equals_each_instance(cuda):
         eng = O.engine_from_model(H, S, blocks=blocks, rtol=1e-12)
         want = eng.moments(phases[i], 40, c[i], a[i])
         assert_rel(got[i], want, 1e-9, f"instance {i}")
+
+
+def test_device_driven_solve_equals_host_polled(cuda):
+    # Engine operations run their solves as captured graphs whose iterations
+    # are a device-driven WHILE node; kmsd_metric_solve polls from the host.
+    # Same kernels and the same iteration rule: the results must be
+    # bit-identical, and the launches inside the device loop must be counted.
+    from tests.gpu_util import engine
+    H, S, blocks = atom_model(40, 21)
+    rng = np.random.default_rng(3)
+    B = rng.standard_normal((S.shape[0], 8)) + 1j * rng.standard_normal((S.shape[0], 8))
+    metric, eng, _ = engine(H, S, blocks=blocks, rtol=1e-12)
+    cfg = metric._create[2]
+    rhs = eng.H.matmul(B)  # H B by the same device SpMM the engine uses
+    host = metric.solve(rhs, cfg)[0]  # host-polled S^-1 (H B)
+    lib = metric.lib
+    before = lib.kmsd_kernel_launches()
+    dev = eng.h_action(B)  # S^-1 H B through the device-driven solve
+    counted = lib.kmsd_kernel_launches() - before
+    np.testing.assert_array_equal(dev, host)
+    assert counted >= 3 * 10  # spmv, update and direction in every iteration
