@@ -402,6 +402,11 @@ enum { S_CSR = 0, S_BSR_REAL = 1, S_BSR_CPLX = 2 };
 // calls this when ks > 1 (the split synchronises the CTA); the dynamic shared
 // memory then holds split_smem_units(MU) double2.
 __host__ __device__ constexpr int split_smem_units(int mu) { return 1024 * mu; }
+// CTAs per SM assumed when the split factor is chosen (block rows x ks up to
+// the row groups of that many CTAs on every SM).
+#ifndef KMSD_SPLIT_CTAS
+#define KMSD_SPLIT_CTAS 4
+#endif
 
 template <int MU, int SF, class XV, class F>
 __device__ __forceinline__ void for_rows_spmv(const CsrView<double> &S, const BsrView<double> &SB, const XV *X,
@@ -1103,7 +1108,7 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
     // rows for the resident row groups (four CTAs per SM)
     int ks = 1;
     if constexpr (SF != S_CSR) {
-        const int64_t resident = (int64_t)sm_count() * 4 * mp.gpc;
+        const int64_t resident = (int64_t)sm_count() * KMSD_SPLIT_CTAS * mp.gpc;
         const int kmax = std::min(8, mp.gpc);
         while (ks * 2 <= kmax && M->S->bsr_nb * ks * 2 <= resident) ks *= 2;
     }
