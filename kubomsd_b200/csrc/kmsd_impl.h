@@ -122,7 +122,8 @@ struct kmsd_metric_s {
     int64_t nblocks = 0;      // 0: diagonal preconditioner
     int *bstart = nullptr;    // device, nblocks+1
     int64_t *foff = nullptr;  // device
-    double2 *factors = nullptr;
+    double2 *factors = nullptr;  // Cholesky factors, or the block inverses (kernels with small blocks)
+    int inv_real = 0;            // factors hold real block inverses
     int maxb = 1;
     int ub = 0;               // uniform block size (block i = rows [i*ub, (i+1)*ub)), else 0
     int store32 = 0;          // CG work vectors stored as complex64 (the mixed form)

@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <type_traits>
 #include <utility>
@@ -62,7 +63,8 @@ struct Pre {
     const int *bstart;
     const int64_t *foff;
     const double2 *factors;
-    int ub;  // uniform block size, or 0: rows and factors are then found without lookups
+    int ub;    // uniform block size, or 0: rows and factors are then found without lookups
+    int real;  // every block inverse is real
 };
 
 __device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
@@ -89,8 +91,18 @@ __device__ __forceinline__ void block_rows(const Pre &P, int64_t bi, int64_t &r0
     }
 }
 
-// z = M^-1 r on one block for one column (native.cpp:259-277 diagonal and
-// block-Jacobi forward/back substitution with the lower Cholesky factor).
+// Blocks of at most this many rows apply the preconditioner as the dense
+// Hermitian inverse (L L^H)^-1, formed once on the host from the Cholesky
+// factor; larger blocks keep the two triangular substitutions.
+#ifndef KMSD_BLOCK_INVERSE
+#define KMSD_BLOCK_INVERSE 8
+#endif
+
+// z = M^-1 r on one block for one column: the diagonal and block-Jacobi
+// preconditioners of native.cpp:259-277.  The reference runs the forward and
+// back substitution with the lower Cholesky factor L; blocks of up to
+// KMSD_BLOCK_INVERSE rows multiply by the stored inverse instead, which is
+// the same operator without divisions or a dependent chain of rows.
 template <int MAXB>
 __device__ __forceinline__ void precond(const Pre &P, int64_t bi, int64_t r0, int m, const double2 (&r)[MAXB],
                                         double2 (&z)[MAXB]) {
@@ -100,7 +112,43 @@ __device__ __forceinline__ void precond(const Pre &P, int64_t bi, int64_t r0, in
         return;
     }
     const double2 *L = P.factors + (P.ub ? bi * P.ub * P.ub : P.foff[bi]);
-    if constexpr (MAXB > 8) {
+    if constexpr (MAXB <= KMSD_BLOCK_INVERSE) {
+        // L holds the inverse, row-major; real when every factor is
+        if (P.real) {
+            const double *Q = reinterpret_cast<const double *>(L);
+#pragma unroll
+            for (int i = 0; i < MAXB; ++i) {
+                if (i < m) {
+                    double2 v = make_double2(0., 0.);
+#pragma unroll
+                    for (int k = 0; k < MAXB; ++k) {
+                        if (k < m) {
+                            const double q = __ldg(Q + 2 * (i * m + k));
+                            v.x += q * r[k].x;
+                            v.y += q * r[k].y;
+                        }
+                    }
+                    z[i] = v;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < MAXB; ++i) {
+                if (i < m) {
+                    double2 v = make_double2(0., 0.);
+#pragma unroll
+                    for (int k = 0; k < MAXB; ++k) {
+                        if (k < m) {
+                            const double2 q = __ldg(L + i * m + k);
+                            v.x += q.x * r[k].x - q.y * r[k].y;
+                            v.y += q.x * r[k].y + q.y * r[k].x;
+                        }
+                    }
+                    z[i] = v;
+                }
+            }
+        }
+    } else {
         // Large blocks: plain loops (registers spill to local memory).
         for (int i = 0; i < m; ++i) {
             double2 v = r[i];
@@ -120,38 +168,6 @@ __device__ __forceinline__ void precond(const Pre &P, int64_t bi, int64_t r0, in
             }
             const double2 d = L[i * m + i];
             z[i] = cdiv(v, make_double2(d.x, -d.y));
-        }
-    } else {
-#pragma unroll
-        for (int i = 0; i < MAXB; ++i) {
-            if (i < m) {
-                double2 v = r[i];
-#pragma unroll
-                for (int k = 0; k < MAXB; ++k) {
-                    if (k < i) {
-                        const double2 l = L[i * m + k];
-                        v.x -= l.x * z[k].x - l.y * z[k].y;
-                        v.y -= l.x * z[k].y + l.y * z[k].x;
-                    }
-                }
-                z[i] = cdiv(v, L[i * m + i]);
-            }
-        }
-#pragma unroll
-        for (int i = MAXB - 1; i >= 0; --i) {
-            if (i < m) {
-                double2 v = z[i];
-#pragma unroll
-                for (int k = 0; k < MAXB; ++k) {
-                    if (k > i && k < m) {
-                        const double2 l = L[k * m + i];  // conj(l) * z[k]
-                        v.x -= l.x * z[k].x + l.y * z[k].y;
-                        v.y -= l.x * z[k].y - l.y * z[k].x;
-                    }
-                }
-                const double2 d = L[i * m + i];
-                z[i] = cdiv(v, make_double2(d.x, -d.y));
-            }
         }
     }
 }
@@ -1144,7 +1160,7 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
     if (mode == kPrepare) return KMSD_OK;
     const int64_t ncols = (int64_t)sv.nseg * b;
     ColPtr c = col_ptr(M->cols.p, ncols);
-    Pre P{M->diag, M->bstart, M->foff, M->factors, M->ub};
+    Pre P{M->diag, M->bstart, M->foff, M->factors, M->ub, M->inv_real};
     const CsrView<double> S = M->S->view64();
     Counters *cnt = M->dcount.as<Counters>();
     double2 *q = M->q.as<double2>(), *y = M->y.as<double2>();
@@ -1519,6 +1535,31 @@ int sample_impl(kmsd_metric_s *M, const double2 *xi, double2 *out, int64_t b, co
     KMSD_CUDA(cudaGetLastError());
     return KMSD_OK;
 }
+// The Hermitian inverse (L L^H)^-1 of one m x m block from its lower
+// Cholesky factor L (row-major): W = L^-1 by forward substitution, then the
+// lower triangle of W^H W, mirrored so that the result is exactly Hermitian
+// with a real diagonal.
+void block_inverse(const double2 *L, int64_t m, double2 *out) {
+    using cd = std::complex<double>;
+    std::vector<cd> W(m * m, cd(0., 0.));
+    auto l = [&](int64_t i, int64_t k) { return cd(L[i * m + k].x, L[i * m + k].y); };
+    for (int64_t j = 0; j < m; ++j) {
+        W[j * m + j] = 1. / l(j, j);
+        for (int64_t i = j + 1; i < m; ++i) {
+            cd v(0., 0.);
+            for (int64_t k = j; k < i; ++k) v += l(i, k) * W[k * m + j];
+            W[i * m + j] = -v / l(i, i);
+        }
+    }
+    for (int64_t i = 0; i < m; ++i)
+        for (int64_t k = 0; k <= i; ++k) {
+            cd v(0., 0.);
+            for (int64_t q = i; q < m; ++q) v += std::conj(W[q * m + i]) * W[q * m + k];
+            if (k == i) v = cd(v.real(), 0.);
+            out[i * m + k] = make_double2(v.real(), v.imag());
+            out[k * m + i] = make_double2(v.real(), -v.imag());
+        }
+}
 }  // namespace
 
 // ------------------------------------------------------------------ ABI
@@ -1564,11 +1605,26 @@ int kmsd_metric_create(kmsd_csr s, const double *diag, int64_t nblocks, const in
             }
         }
     }
+    // Kernels for blocks of up to KMSD_BLOCK_INVERSE rows (the 4- and 8-row
+    // instantiations) multiply by the block inverses.
+    const int bucket = maxb <= 1 ? 1 : maxb <= 4 ? 4 : maxb <= 8 ? 8 : 32;
+    bool inv_real = false;
+    if (nblocks > 0 && bucket > 1 && bucket <= KMSD_BLOCK_INVERSE) {
+        std::vector<double2> inv(fac.size(), make_double2(0., 0.));
+        for (int64_t i = 0; i < nblocks; ++i)
+            block_inverse(fac.data() + offs[i], block_start[i + 1] - block_start[i], inv.data() + offs[i]);
+        for (const double2 &v : inv)
+            if (!std::isfinite(v.x) || !std::isfinite(v.y))
+                return fail(KMSD_EINVAL, "invalid block-Jacobi factor partition");
+        inv_real = std::all_of(inv.begin(), inv.end(), [](const double2 &v) { return v.y == 0.; });
+        fac.swap(inv);
+    }
     auto *M = new kmsd_metric_s();
     M->S = s;
     M->n = n;
     M->nblocks = nblocks;
     M->maxb = maxb;
+    M->inv_real = inv_real;
     M->bstart_host.assign(bs.begin(), bs.end());
     // Uniform partition with factors packed in block order (atom blocks of
     // one size): the kernels then compute rows and factor offsets directly.
