@@ -128,3 +128,57 @@ def test_block_sparse_spmm_and_solve(cuda, cplx):
     assert rep.converged.all()
     ref = spla.spsolve(S.tocsc(), X)
     assert_rel(y, ref, 1e-10, "block-sparse metric solve")
+
+
+def _hermitian_blocks(sizes, seed, coupling=0.):
+    """A complex Hermitian positive definite S whose diagonal blocks have the
+    given sizes, plus an optional sparse Hermitian coupling between them
+    (diagonally shifted so that S stays positive definite)."""
+    rng = np.random.default_rng(seed)
+    off = np.cumsum([0] + list(sizes))
+    n = int(off[-1])
+    S = np.zeros((n, n), complex)
+    for a, b in zip(off[:-1], off[1:]):
+        X = rng.standard_normal((b - a, b - a)) + 1j * rng.standard_normal((b - a, b - a))
+        S[a:b, a:b] = X @ X.conj().T / (b - a) + np.eye(b - a)
+    if coupling:
+        C = coupling * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+        C = np.where(rng.random((n, n)) < .2, C, 0.)
+        C = np.triu(C, 1)
+        C = C + C.conj().T
+        S += C + np.diag(np.abs(C).sum(axis=1))
+    return S, off
+
+
+@pytest.mark.parametrize("sizes", [(1, 2, 5, 8, 3, 4, 7, 6), (12, 9, 4, 1, 10)])
+def test_block_jacobi_of_a_block_diagonal_metric_is_exact(cuda, sizes):
+    # Blocks of up to 8 rows are applied as stored block inverses, larger
+    # ones by substitution with the Cholesky factor: either way M^-1 = S^-1
+    # here, so one iteration converges.
+    import scipy.linalg as la
+    S, off = _hermitian_blocks(sizes, 40 + len(sizes))
+    blocks = [(int(a), int(b), la.cholesky(S[a:b, a:b], lower=True)) for a, b in zip(off[:-1], off[1:])]
+    m, cfg = metric(S, blocks)
+    rng = np.random.default_rng(3)
+    B = rng.standard_normal((S.shape[0], 3)) + 1j * rng.standard_normal((S.shape[0], 3))
+    y, rep = m.solve(B, cfg)
+    assert rep.iterations.tolist() == [1, 1, 1] and rep.converged.all()
+    assert_rel(y, np.linalg.solve(S, B), 1e-12, "solution")
+
+
+@pytest.mark.parametrize("sizes", [(1, 2, 5, 8, 3, 4, 7, 6) * 3, (12, 9, 4, 1, 10) * 2])
+def test_block_jacobi_on_a_coupled_complex_metric(cuda, sizes):
+    import scipy.linalg as la
+    S, off = _hermitian_blocks(sizes, 50 + len(sizes), coupling=.05)
+    blocks = [(int(a), int(b), la.cholesky(S[a:b, a:b], lower=True)) for a, b in zip(off[:-1], off[1:])]
+    m, cfg = metric(S, blocks, rtol=1e-12)
+    md, _ = metric(S, (), rtol=1e-12)
+    rng = np.random.default_rng(4)
+    B = rng.standard_normal((S.shape[0], 5)) + 1j * rng.standard_normal((S.shape[0], 5))
+    y, rep = m.solve(B, cfg)
+    yd, repd = md.solve(B, cfg)
+    assert rep.converged.all() and repd.converged.all()
+    want = np.linalg.solve(S, B)
+    assert_rel(y, want, 1e-10, "block-Jacobi solution")
+    assert_rel(yd, want, 1e-10, "diagonal solution")
+    assert rep.iterations.max() <= repd.iterations.max()  # the blocks precondition at least as well
