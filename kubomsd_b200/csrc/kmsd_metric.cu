@@ -497,7 +497,21 @@ __device__ __forceinline__ void for_rows_spmv(const CsrView<double> &S, const Bs
 struct Loop {
     int on, maxiter;
     cudaGraphConditionalHandle again, check;
+    int has_check;  // the check kernels sit in an IF node driven by `check`
 };
+
+// Launch options of the device-driven loop body: KMSD_PCG_PDL chains the
+// body's kernels with programmatic dependent launch (a kernel's CTAs are
+// scheduled while its predecessor drains and wait in griddepcontrol.wait
+// until it has completed); KMSD_PCG_IFNODE = 0 runs the true-residual and
+// restart kernels in every iteration (they return at once unless a check is
+// due) instead of behind an IF node.
+#ifndef KMSD_PCG_PDL
+#define KMSD_PCG_PDL 1
+#endif
+#ifndef KMSD_PCG_IFNODE
+#define KMSD_PCG_IFNODE 1
+#endif
 
 // Kernels launched inside device-driven loops, counted on the device (the
 // host does not see those launches).
@@ -505,6 +519,9 @@ __device__ unsigned long long g_loop_launches;
 
 __device__ __forceinline__ void loop_count(const Loop &lp) {
     if (lp.on && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&g_loop_launches, 1ull);
+    // (no-ops unless launched as a programmatic dependent)
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
 }
 
 // ---- sp = S p, curvature <p, sp>, alpha, breakdown
@@ -687,7 +704,7 @@ __global__ void __launch_bounds__(256, KMSD_PCG_MINB(MAXB))
             if (lp.on) {
                 const int k = c.flags[5] + 1;
                 c.flags[5] = k;
-                cudaGraphSetConditional(lp.check, c.flags[1] ? 1u : 0u);
+                if (lp.has_check) cudaGraphSetConditional(lp.check, c.flags[1] ? 1u : 0u);
                 cudaGraphSetConditional(lp.again, (c.flags[0] == 0 && k < lp.maxiter) ? 1u : 0u);
             }
         }
@@ -1112,6 +1129,23 @@ namespace {
 // nothing), or from the device as the WHILE node of a capturing stream.
 enum { kHostLoop = 0, kPrepare = 1, kDeviceLoop = 2 };
 
+// A kernel launch, as a programmatic dependent of the stream's previous
+// kernel when `pdl` is set.
+template <class... KArgs, class... Args>
+cudaError_t launch_k(bool pdl, void (*kernel)(KArgs...), int grid, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 template <int MU, int MAXB, int SF, bool SEG, class W>
 int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rtol, double atol, int maxiter,
             cudaStream_t s, int *status, FailReportFull *fr, int *claimed, int mode) {
@@ -1201,40 +1235,57 @@ int run_pcg(kmsd_metric_s *M, const double2 *B, double2 *Y, int64_t b, double rt
         KMSD_CUDA(cudaGraphAddNode(&wnode, g, deps, nd, &wp));
         KMSD_CUDA(cudaStreamUpdateCaptureDependencies(s, &wnode, 1, cudaStreamSetCaptureDependencies));
         cudaGraph_t body = wp.conditional.phGraph_out[0];
-        KMSD_CUDA(cudaGraphConditionalHandleCreate(&lp.check, body, 0, cudaGraphCondAssignDefault));
+        // (the IF handle goes into the update kernel's arguments, so it is made first)
+        lp.has_check = KMSD_PCG_IFNODE;
+        if (KMSD_PCG_IFNODE) KMSD_CUDA(cudaGraphConditionalHandleCreate(&lp.check, body, 0, cudaGraphCondAssignDefault));
         cudaStream_t bs = M->loop_stream, cs2 = M->check_stream;
         KMSD_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        pcg_spmv_kernel<MU, SF, SEG><<<grid_s, kThreads, sm_s, bs>>>(S, SB, p, sp, n, mp, c, part, tk, sv, lp, ks);
-        pcg_update_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, bs>>>(y, r, z, p, sp, P, nb, mp, c, 0, M->interval,
-                                                                       M->adaptive, part, tk, sv, lp);
-        cudaError_t le = cudaGetLastError();
-        cudaStreamCaptureStatus bcs;
-        cudaGraph_t bg = nullptr;
-        const cudaGraphNode_t *bdeps = nullptr;
-        size_t bnd = 0;
-        cudaGraphNode_t inode = nullptr;
-        cudaError_t ae = cudaStreamGetCaptureInfo(bs, &bcs, nullptr, &bg, &bdeps, &bnd);
-        if (ae == cudaSuccess) {
-            ip.type = cudaGraphNodeTypeConditional;
-            ip.conditional.handle = lp.check;
-            ip.conditional.type = cudaGraphCondTypeIf;
-            ip.conditional.size = 1;
-            ae = cudaGraphAddNode(&inode, bg, bdeps, bnd, &ip);
+        cudaError_t le = launch_k(false, pcg_spmv_kernel<MU, SF, SEG, W>, grid_s, sm_s, bs, S, SB, (const W *)p, sp,
+                                  n, mp, c, part, tk, sv, lp, ks);
+        if (le == cudaSuccess)
+            le = launch_k(KMSD_PCG_PDL, pcg_update_kernel<MU, MAXB, SEG, W>, grid_b, sm, bs, y, r, z, (const W *)p,
+                          (const W *)sp, P, nb, mp, c, 0, M->interval, M->adaptive, part, tk, sv, lp);
+        cudaError_t ae = cudaSuccess;
+        if (KMSD_PCG_IFNODE) {
+            cudaStreamCaptureStatus bcs;
+            cudaGraph_t bg = nullptr;
+            const cudaGraphNode_t *bdeps = nullptr;
+            size_t bnd = 0;
+            cudaGraphNode_t inode = nullptr;
+            ae = cudaStreamGetCaptureInfo(bs, &bcs, nullptr, &bg, &bdeps, &bnd);
+            if (ae == cudaSuccess) {
+                ip.type = cudaGraphNodeTypeConditional;
+                ip.conditional.handle = lp.check;
+                ip.conditional.type = cudaGraphCondTypeIf;
+                ip.conditional.size = 1;
+                ae = cudaGraphAddNode(&inode, bg, bdeps, bnd, &ip);
+            }
+            if (ae == cudaSuccess)
+                ae = cudaStreamUpdateCaptureDependencies(bs, &inode, 1, cudaStreamSetCaptureDependencies);
+            if (ae == cudaSuccess)
+                ae = cudaStreamBeginCaptureToGraph(cs2, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                   cudaStreamCaptureModeThreadLocal);
+            if (ae == cudaSuccess) {
+                pcg_true_residual_kernel<MU, SF, SEG><<<grid_s, kThreads, sm_s, cs2>>>(
+                    S, SB, q, y, r, t, n, mp, c, M->adaptive, M->gap_ratio, part, tk, cnt, sv, lp, ks);
+                pcg_restart_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, cs2>>>(r, z, t, P, nb, mp, c, part, tk, sv,
+                                                                                lp);
+                if (le == cudaSuccess) le = cudaGetLastError();
+                cudaGraph_t ib = nullptr;
+                ae = cudaStreamEndCapture(cs2, &ib);
+            }
+        } else {
+            if (le == cudaSuccess)
+                le = launch_k(KMSD_PCG_PDL, pcg_true_residual_kernel<MU, SF, SEG, W>, grid_s, sm_s, bs, S, SB,
+                              (const double2 *)q, (const double2 *)y, (const W *)r, t, n, mp, c, M->adaptive,
+                              M->gap_ratio, part, tk, cnt, sv, lp, ks);
+            if (le == cudaSuccess)
+                le = launch_k(KMSD_PCG_PDL, pcg_restart_kernel<MU, MAXB, SEG, W>, grid_b, sm, bs, r, z,
+                              (const W *)t, P, nb, mp, c, part, tk, sv, lp);
         }
-        if (ae == cudaSuccess) ae = cudaStreamUpdateCaptureDependencies(bs, &inode, 1, cudaStreamSetCaptureDependencies);
-        if (ae == cudaSuccess)
-            ae = cudaStreamBeginCaptureToGraph(cs2, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                               cudaStreamCaptureModeThreadLocal);
-        if (ae == cudaSuccess) {
-            pcg_true_residual_kernel<MU, SF, SEG><<<grid_s, kThreads, sm_s, cs2>>>(
-                S, SB, q, y, r, t, n, mp, c, M->adaptive, M->gap_ratio, part, tk, cnt, sv, lp, ks);
-            pcg_restart_kernel<MU, MAXB, SEG><<<grid_b, kThreads, sm, cs2>>>(r, z, t, P, nb, mp, c, part, tk, sv, lp);
-            if (le == cudaSuccess) le = cudaGetLastError();
-            cudaGraph_t ib = nullptr;
-            ae = cudaStreamEndCapture(cs2, &ib);
-        }
-        pcg_direction_kernel<SEG><<<egrid, 256, 0, bs>>>(z, p, len, mp, c, sv, lp);
-        if (le == cudaSuccess) le = cudaGetLastError();
+        if (le == cudaSuccess)
+            le = launch_k(KMSD_PCG_PDL && !KMSD_PCG_IFNODE, pcg_direction_kernel<SEG, W>, egrid, 0, bs, z, p, len,
+                          mp, c, sv, lp);
         cudaGraph_t bout = nullptr;
         const cudaError_t ee = cudaStreamEndCapture(bs, &bout);
         if (ae != cudaSuccess) return cuda_fail(ae, "device PCG loop (check branch)");
