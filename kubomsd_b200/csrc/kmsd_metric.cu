@@ -525,8 +525,19 @@ __device__ __forceinline__ void loop_count(const Loop &lp) {
 }
 
 // ---- sp = S p, curvature <p, sp>, alpha, breakdown
+// CTAs per SM the S-product kernel is compiled for (one unit per lane); 0:
+// left to the compiler.
+#ifndef KMSD_SPMV_MINB
+#define KMSD_SPMV_MINB 0
+#endif
+#if KMSD_SPMV_MINB > 0
+#define KMSD_SPMV_BOUNDS(mu) __launch_bounds__(256, (mu) == 1 ? KMSD_SPMV_MINB : 1)
+#else
+#define KMSD_SPMV_BOUNDS(mu) __launch_bounds__(256)
+#endif
+
 template <int MU, int SF, bool SEG, class W>
-__global__ void __launch_bounds__(256)
+__global__ void KMSD_SPMV_BOUNDS(MU)
     pcg_spmv_kernel(CsrView<double> S, BsrView<double> SB, const W *p, W *sp, int64_t n, RowMap mp,
                     ColPtr c, double2 *partial, Ticket *tk, SegView sv, Loop lp, int ks) {
     loop_count(lp);
