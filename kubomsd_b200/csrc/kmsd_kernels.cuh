@@ -137,18 +137,28 @@ __device__ __forceinline__ void gather_block_row(const BsrView<double> &A, const
                                                  int G, int lane, Pk<double> (&acc)[4][MU], int part = 0,
                                                  int ks = 1) {
     const int k0 = __ldg(A.bptr + I) + part, k1 = __ldg(A.bptr + I + 1);
+    // Lanes past the last unit read the last unit instead: their sums are
+    // never stored, and the gathers need no per-load select.
+    const XV *xl[MU];
+#pragma unroll
+    for (int m = 0; m < MU; ++m) {
+        const int u = lane + m * G;
+        xl[m] = X + (u < U ? u : U - 1);
+    }
+    const unsigned U4 = 4u * (unsigned)U;
+    const size_t Us = (size_t)U;
     // the next block's column index is loaded one block ahead, so each
     // block's gathers wait for one memory round trip, not two
     int Jn = k0 < k1 ? __ldg(A.bidx + k0) : 0;
     for (int k = k0; k < k1; k += ks) {
-        const int J = Jn;
+        const unsigned J = (unsigned)Jn;
         if (k + ks < k1) Jn = __ldg(A.bidx + k + ks);
         Pk<double> x[MU][4];
 #pragma unroll
         for (int m = 0; m < MU; ++m) {
-            const int u = lane + m * G;
+            const XV *xr = xl[m] + (size_t)J * U4;  // block column J: rows 4J .. 4J+3
 #pragma unroll
-            for (int j = 0; j < 4; ++j) x[m][j] = u < U ? ldg_d(X + (size_t)(4 * J + j) * U + u) : pk_zero<double>();
+            for (int j = 0; j < 4; ++j) x[m][j] = ldg_d(xr + j * Us);
         }
         const double2 *pr = reinterpret_cast<const double2 *>(A.re + (size_t)k * 16);
 #pragma unroll

@@ -528,7 +528,7 @@ __device__ __forceinline__ void loop_count(const Loop &lp) {
 // CTAs per SM the S-product kernel is compiled for (one unit per lane); 0:
 // left to the compiler.
 #ifndef KMSD_SPMV_MINB
-#define KMSD_SPMV_MINB 0
+#define KMSD_SPMV_MINB 4
 #endif
 #if KMSD_SPMV_MINB > 0
 #define KMSD_SPMV_BOUNDS(mu) __launch_bounds__(256, (mu) == 1 ? KMSD_SPMV_MINB : 1)
