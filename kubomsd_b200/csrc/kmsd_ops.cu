@@ -10,11 +10,14 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <type_traits>
 #include <vector>
 
 #include "kmsd.h"
 #include "kmsd_impl.h"
 #include "kmsd_kernels.cuh"
+#include "kmsd_tile.cuh"
 
 using namespace kmsd;
 
@@ -55,6 +58,7 @@ int finish(E *e, cudaStream_t s) {
         }
     }
     if (st[2] != 0) return fail(KMSD_ERUNTIME, "nonfinite Chebyshev propagation; check bounds and solves");
+    if (st[3] != 0) return fail(KMSD_ERUNTIME, "a bounded device wait of the tiled Chebyshev step ran out");
     return KMSD_OK;
 }
 
@@ -169,12 +173,76 @@ int launch_step_h(E *e, StepArgs<T> &a, cudaStream_t s) {
     return fail(KMSD_EINVAL, "too many columns for one engine call");
 }
 
+// Tile-pipelined moment step (kmsd_tile.cuh): persistent grid of one
+// resident wave; tiles sized so the stage ring of a CTA is about
+// KMSD_TILE_RING bytes, a whole number of rows per row group.
+template <class T, int MODE, int W>
+int launch_tile(E *e, StepArgs<T> &a, cudaStream_t s) {
+    const auto kern = cheb_tile_kernel<T, MODE, W>;
+    static int smem_cap = 0;  // per instantiation
+    if (!smem_cap) {
+        int dev = 0, optin = 0;
+        KMSD_CUDA(cudaGetDevice(&dev));
+        KMSD_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        KMSD_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       optin - 1024));
+        smem_cap = optin - 1024;
+    }
+    const RowMap &mp = a.mp;
+    const int nvec = MODE == MODE_DIRECT ? 3 : 2;
+    const int row_bytes = nvec * mp.U * 16 + W * (4 + (int)sizeof(T));
+    int tr = KMSD_TILE_RING / KMSD_TILE_STAGES / row_bytes / mp.gpc * mp.gpc;
+    tr = std::max(mp.gpc, std::min(kTileMaxRows / mp.gpc * mp.gpc, tr));
+    const TileLayout L = tile_layout(tr, mp.U, W, nvec, (int)sizeof(T));
+    const size_t sm = tile_smem(L, mp, Unit<T>::C);
+    if (sm > (size_t)smem_cap) return fail(KMSD_EINVAL, "tile step does not fit in shared memory");
+    static std::map<size_t, int> per_sm_cache;  // per instantiation: shared bytes -> CTAs per SM
+    int per_sm = 0;
+    auto it = per_sm_cache.find(sm);
+    if (it != per_sm_cache.end()) {
+        per_sm = it->second;
+    } else {
+        KMSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)kern, kTileThreads, sm));
+        per_sm = std::max(per_sm, 1);
+        per_sm_cache[sm] = per_sm;
+    }
+    const int64_t ntiles = (a.n + tr - 1) / tr;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)sm_count() * per_sm));
+    if (e->red.ensure(grid, mp.U * Unit<T>::C, 2)) return KMSD_ECUDA;
+    a.partial = e->red.part();
+    a.ticket = e->red.tick();
+    kern<<<grid, kTileThreads, sm, s>>>(a, L, status_ptr(e) + 3);
+    return KMSD_OK;
+}
+
+inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// The tile step applies to moment steps over a real ELL form of width 4 or 8
+// with one unit per lane, on 16-byte aligned operands.
+template <class T, int MODE, bool IH>
+bool tile_applies(const StepArgs<T> &a) {
+    if (!KMSD_TILE || !IH || (MODE != MODE_DOUBLING && MODE != MODE_DIRECT)) return false;
+    if (std::is_same<T, float>::value && MODE == MODE_DOUBLING && !KMSD_TILE_F32_DOUBLING) return false;
+    if (a.E.im != nullptr || (a.E.w != 4 && a.E.w != 8) || a.mp.U > 128 || mu_for(a.mp) != 1) return false;
+    return aligned16(a.curr) && aligned16(a.prev) && aligned16(a.next) &&
+           (MODE != MODE_DIRECT || aligned16(a.bra));
+}
+
 // IH: the operator is applied inline (identity metric), from the ELL form
 // when the matrix has one, else from CSR; otherwise the step reads the solved
 // operand a.hx.
 template <class T, int MODE, bool IH, bool IV>
 int launch_step(E *e, StepArgs<T> &a, cudaStream_t s) {
     int rc;
+    if constexpr (MODE == MODE_DOUBLING || MODE == MODE_DIRECT) {
+        if (tile_applies<T, MODE, IH>(a)) {
+            rc = a.E.w == 4 ? launch_tile<T, MODE, 4>(e, a, s) : launch_tile<T, MODE, 8>(e, a, s);
+            if (rc) return rc;
+            count_launch();
+            KMSD_CUDA(cudaGetLastError());
+            return KMSD_OK;
+        }
+    }
     if (!IH) rc = launch_step_h<T, MODE, HSRC_SOLVED, IV>(e, a, s);
     else if (a.E.w == 4 && a.E.im == nullptr) rc = launch_step_h<T, MODE, HSRC_ELL4, IV>(e, a, s);
     else if (a.E.w == 8 && a.E.im == nullptr) rc = launch_step_h<T, MODE, HSRC_ELL8, IV>(e, a, s);
