@@ -6,8 +6,9 @@
 # the output directory is git-ignored.  Used only by tests/, the oracle checks
 # and bench.py's CPU baseline arm.
 set -euo pipefail
-REF="${KUBOMSD_REFERENCE:-/root/reference}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+# the reference checkout: $KUBOMSD_REFERENCE, else `reference` beside the repository
+REF="${KUBOMSD_REFERENCE:-$(dirname "$(dirname "$HERE")")/reference}"
 OUT="$HERE/_ref"
 SRC="$REF/cpp/native.cpp"
 if [[ ! -f "$SRC" ]]; then

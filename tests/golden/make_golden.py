@@ -5,11 +5,16 @@ stepwise_samples, iter_stochastic_blocks, ...) on top of its compiled CPU
 engine cpp/native.cpp, built into oracle/_ref/ by oracle/build_ref.sh, with
 `cpu_kernel="cpp"` — the reference's production CPU path.  The outputs are
 stored as small .npz files together with their inputs; tests compare the B200
-engine and the oracle restatement against them.  Needs the reference checkout
-(default /root/reference, or $KUBOMSD_REFERENCE); h5py is not needed because
-only the solver layer is driven.
+engine and the oracle restatement against them.  Needs the reference checkout:
+$KUBOMSD_REFERENCE, else a directory named `reference` beside this
+repository; h5py is not needed because only the solver layer is driven.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every case
+    python tests/golden/make_golden.py c3_fp64    # named cases only
+
+The stated-configuration cases (c1_square64_full, c3_honeycomb_fp64,
+c2_diamond10) run the full-size lattices of the precision form and the
+nonorthogonal model at reduced moment and vector counts; they take minutes.
 """
 from __future__ import annotations
 
@@ -25,7 +30,7 @@ import scipy.sparse as sp
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
-REF = Path(os.environ.get("KUBOMSD_REFERENCE", "/root/reference"))
+REF = Path(os.environ.get("KUBOMSD_REFERENCE", ROOT.parent / "reference"))
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(REF / "src"))
 sys.path.insert(0, str(REF))
@@ -36,6 +41,9 @@ ref_native.build()
 import kubo_msd  # noqa: E402
 
 kubo_msd.__path__.append(str(ref_native.REF_DIR))  # kubo_msd._native from oracle/_ref
+import kubo_msd._native  # noqa: E402
+
+ref_native._module = kubo_msd._native  # one registration of the pybind classes for both routes
 
 from kubo_msd.config import RunConfig  # noqa: E402
 from kubo_msd.contracts import ModelBundle  # noqa: E402
@@ -276,22 +284,89 @@ def diamond_case():
     return out
 
 
-def main():
-    cases = {}
-    for kind in ("velocity", "position", "composite"):
-        for pre in ("diagonal", "block-jacobi"):
-            cases[f"engine_{kind}_{pre}"] = engine_case(kind, pre)
-    cases["pcg_known"] = pcg_known()
-    cases["host_formulas"] = host_formulas()
-    cases["square16_pipeline"] = square_pipeline()
-    cases["square16_pipeline_vac"] = square_pipeline("stepwise", include_vac=True)
-    cases["square16_pipeline_spectral"] = square_pipeline("spectral", include_vac=False)
-    cases["c1_square64"] = c1_case()
-    cases["diamond2"] = diamond_case()
-    for name, arrays in cases.items():
+def c1_full_case():
+    """Config 1 in full: 64x64 square lattice, R=8, M=512, 201 energies,
+    stepwise MSD along x over 0-50 fs at dt = 1 fs, no VAC."""
+    m = lattices.square_lattice(64)
+    model = ModelBundle(m.H, m.S, velocity=m.velocity)
+    cfg = RunConfig(energy_eV=np.linspace(-11, 11, 201), time_fs=np.arange(51.), solver="stochastic-kpm",
+                    kernel="jackson", axes=("x",), spectral_bounds=(-11.2, 11.2), n_moments=512,
+                    include_vac=False, stochastic_method="stepwise", cpu_kernel="cpp", omp_threads=OMP)
+    ops = build_operators(model, cfg)
+    B = random_phases(m.n, 20261019, range(8))
+    dos, nums, diag = stepwise_samples(ops, cfg, B)
+    return {"H_digest": np.array(digest(m.H)), "V_digest": np.array(digest(m.velocity["x"])), "dos": dos,
+            "msd": nums["msd_A2/commutator"], "time_fs": np.asarray(cfg.time_fs)}
+
+
+def c3_fp64_case():
+    """Precision-form lattice at full size: honeycomb 2048 x 1024 cells x 2 =
+    4,194,304 sites, W = 1 eV; the reference engine's FP64 moments
+    (Engine::moments, cpp/native.cpp:590-609) of R=8 phase vectors (sample ids
+    0..7, seed 20261019), M=16, window (-9.2, 9.2) eV."""
+    m = lattices.honeycomb(2048, 1024, with_velocity=False)
+    eng = ref_native.RefEngine(m.H, sp.identity(m.n, format="csr"), threads=OMP)
+    B = random_phases(m.n, 20261019, range(8))
+    c, a = 0., 9.2
+    return {"H_digest": np.array(digest(m.H)), "moments": eng.core.moments(B, 16, c, a), "center": c, "half": a}
+
+
+def c2_full_case():
+    """Config-2 model at full size: diamond sp3, 10^3 cells x 8 atoms x 4
+    orbitals = 32,000 orbitals, kappa(S) = 50, block-Jacobi PCG.  The solves
+    are tightened to rtol 1e-12 (the reference's own parity tests tighten
+    theirs to 2e-13) so that solve tolerance does not mask the comparison.
+    S^-1/2 sampling of R=4 phases, M=8 moments, v_cov along x, and a short
+    stepwise MSD (x, y, z; 0, 0.5, 1 fs; M=16) of R=2 vectors."""
+    m = lattices.diamond_sp3(cells=10)
+    model = ModelBundle(m.H, m.S, composite=m.composite, atom_slices=m.atom_slices)
+    cfg = RunConfig(energy_eV=np.linspace(-30, 30, 13), time_fs=[0., .5, 1.], solver="stochastic-kpm",
+                    kernel="jackson", axes=("x", "y", "z"), spectral_bounds=(-40., 40.), n_moments=16,
+                    include_vac=False, stochastic_method="stepwise", cpu_kernel="cpp", metric_rtol=1e-12,
+                    preconditioner="block-jacobi", segment_fs=.5, omp_threads=OMP)
+    ops = build_operators(model, cfg)
+    sampler = MetricSampler(ops.metric, cfg)
+    xi = random_phases(m.n, 20261019, range(4))
+    c, a = scaling(cfg)
+    out = {"H_digest": np.array(digest(m.H)), "S_digest": np.array(digest(m.S)),
+           "sample_coeff": np.asarray(sampler.coeff), "sample_center": sampler.center,
+           "sample_half": sampler.half}
+    out["sample"] = sampler.transform(xi)
+    out["moments"] = ops.native.moments(xi, 8, c, a)
+    out["v_cov_x"] = ops.native.v_cov([1., 0., 0.], xi[:, :2])
+    dos, nums, _ = stepwise_samples(ops, cfg, xi[:, :2])
+    out["dos"] = dos
+    out["msd"] = nums["msd_A2/commutator"]
+    return out
+
+
+OMP = os.cpu_count() or 1
+
+CASES = {
+    **{f"engine_{kind}_{pre}": (lambda kind=kind, pre=pre: engine_case(kind, pre))
+       for kind in ("velocity", "position", "composite") for pre in ("diagonal", "block-jacobi")},
+    "pcg_known": pcg_known,
+    "host_formulas": host_formulas,
+    "square16_pipeline": square_pipeline,
+    "square16_pipeline_vac": lambda: square_pipeline("stepwise", include_vac=True),
+    "square16_pipeline_spectral": lambda: square_pipeline("spectral", include_vac=False),
+    "c1_square64": c1_case,
+    "diamond2": diamond_case,
+    "c1_square64_full": c1_full_case,
+    "c3_honeycomb_fp64": c3_fp64_case,
+    "c2_diamond10": c2_full_case,
+}
+
+
+def main(names):
+    import time
+    for name in names or CASES:
+        t0 = time.perf_counter()
+        arrays = CASES[name]()
         np.savez_compressed(HERE / f"{name}.npz", **arrays)
-        print(name, sum(np.asarray(v).nbytes for v in arrays.values()), "bytes")
+        print(name, sum(np.asarray(v).nbytes for v in arrays.values()), "bytes",
+              f"{time.perf_counter() - t0:.1f} s", flush=True)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -49,3 +49,20 @@ def test_batch_tuner_keeps_results(instances):
     rows = bt.tune(blocks[:5], 64, c, a)
     assert rows in (512, 1024, 2048, 4096, 8192)
     assert_rel(bt.moments(blocks[:5], 64, c, a).cpu().numpy(), before, 1e-12, "after tuning")
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_moments_match_oracle_per_instance(instances, precision):
+    """Each instance of the orthogonal batch against the oracle's Engine::moments
+    (cpp/native.cpp:590-609 restated): 1e-10 in FP64, the stated moment
+    tolerance (5e-5, norm-wise) in the mixed form."""
+    from kubomsd_b200.batch import B200Batch
+    from oracle import kpm_oracle as O
+    ms, blocks, bounds = instances
+    bt = B200Batch([m.H for m in ms], precision=precision, tile_rows=1024)
+    c = [(lo + hi) / 2 for lo, hi in bounds]
+    a = [(hi - lo) / 2 for lo, hi in bounds]
+    got = bt.moments(blocks, 96, c, a, doubling=True).cpu().numpy()
+    for i, m in enumerate(ms):
+        want = O.engine_from_model(m.H, m.S).moments(blocks[i], 96, c[i], a[i])
+        assert_rel(got[i], want, 1e-10 if precision == "fp64" else 5e-5, f"instance {i} vs oracle")
