@@ -337,6 +337,21 @@ def c2_full_case():
     dos, nums, _ = stepwise_samples(ops, cfg, xi[:, :2])
     out["dos"] = dos
     out["msd"] = nums["msd_A2/commutator"]
+    return compact_rows(out, ("sample", "v_cov_x"))
+
+
+ROW_STRIDE = 16
+
+
+def compact_rows(out, names):
+    """Keeps the fixture small: for each (N, b) array, every ROW_STRIDE-th row
+    plus the whole array's column sums and column norms."""
+    for name in names:
+        full = np.asarray(out.pop(name))
+        out[name + "_rows"] = full[::ROW_STRIDE]
+        out[name + "_colsum"] = full.sum(axis=0)
+        out[name + "_colnorm"] = np.linalg.norm(full, axis=0)
+    out["row_stride"] = np.array(ROW_STRIDE)
     return out
 
 
