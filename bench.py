@@ -67,6 +67,9 @@ def parse():
                         "arithmetic, solution, inner products and tests)")
     p.add_argument("--no-compare", action="store_true", help="skip the FP64 / direct comparison lines")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip the per-configuration blocks (config 1 in full, config 2 at full size, a config-5 "
+                        "serving window)")
     return p.parse_args()
 
 
@@ -133,28 +136,57 @@ def dist_setup(args):
     return world, rank, local
 
 
-def cpu_baseline(H, n, threads, R=8, M=4):
-    """KuboMSD's compiled CPU engine (oracle/_ref) on a bounded sample of the workload."""
+M_FULL = 4096
+
+
+def _ref_engine(H, S, threads, **kw):
+    """KuboMSD's compiled CPU engine (oracle/_ref), or None when it is absent."""
     from oracle import ref_native
+    if ref_native.load() is None:
+        return None
+    return ref_native.RefEngine(H, S, threads=threads, **kw)
+
+
+def time_applications(run, steps=1):
+    """Seconds of the set-up part (M=1: S B and mu_0) and of one operator
+    application (an M=2 call minus the set-up) of a moments call `run(M)`."""
+    t0 = time.perf_counter()
+    run(1)
+    t1 = time.perf_counter() - t0
+    t2 = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        run(2)
+        t2.append(time.perf_counter() - t0)
+    t2 = min(t2)
+    return t1, max(t2 - t1, 1e-9), t2
+
+
+def cpu_baseline(H, n, threads, R=64, M=M_FULL, setup=None):
+    """KuboMSD's compiled CPU engine (oracle/_ref) on a bounded sample of the
+    moments workload: one M=1 call (S B and mu_0) and one M=2 call (one
+    operator application) on the full lattice with all R vectors; the M-moment
+    call is extrapolated as set-up + (M - 1) applications, which is exactly
+    the work Engine::moments does (cpp/native.cpp:590-609)."""
     import scipy.sparse as sp
-    mod = ref_native.load()
-    kind = "reference"
     B = np.exp(2j * np.pi * np.random.default_rng(9).random((n, R)))
     c, a = (BOUNDS[0] + BOUNDS[1]) / 2, (BOUNDS[1] - BOUNDS[0]) / 2
-    if mod is not None:
-        eng = ref_native.RefEngine(H, sp.identity(n, format="csr"), threads=threads)
-        run = lambda: eng.core.moments(B, M, c, a)  # noqa: E731
+    eng = _ref_engine(H, sp.identity(n, format="csr"), threads)
+    kind = "reference"
+    if eng is not None:
+        run = lambda m: eng.core.moments(B, m, c, a)  # noqa: E731
     else:  # the oracle restatement when the reference binary is absent
         from oracle import kpm_oracle as O
-        eng = O.engine_from_model(H, sp.identity(n, format="csr"))
-        run = lambda: eng.moments(B, M, c, a)  # noqa: E731
+        oe = O.engine_from_model(H, sp.identity(n, format="csr"))
+        run = lambda m: oe.moments(B, m, c, a)  # noqa: E731
         kind, threads = "port", 1
-    t0 = time.perf_counter()
-    run()
-    dt = time.perf_counter() - t0
-    return {"value": n * M * R / dt, "unit": UNIT, "cores": threads, "kind": kind, "seconds": dt,
-            "sample": f"one moments call, R={R} vectors, M={M} moments on the full {n:,}-site lattice "
-                      f"({threads} OpenMP threads)"}
+    t_setup, t_app, t_call = time_applications(run)
+    full = t_setup + (M - 1) * t_app
+    return {"value": n * M * R / full, "unit": UNIT, "cores": threads, "kind": kind, "seconds": t_setup + t_call,
+            "applications_per_s": n * R / t_app, "seconds_per_application": t_app, "setup_seconds": t_setup,
+            "sample": f"Engine::moments on the full {n:,}-site lattice with R={R} vectors: one M=1 call "
+                      f"(set-up {t_setup:.2f} s) and one M=2 call (one operator application, {t_app:.2f} s), "
+                      f"{threads} OpenMP threads; the M={M} call extrapolated as set-up + {M - 1} applications"}
 
 
 def run_reference(args):
@@ -162,23 +194,300 @@ def run_reference(args):
     if rank != 0:
         return
     from kubomsd_b200 import lattices
+    import scipy.sparse as sp
     m = lattices.honeycomb(args.lx, args.ly, with_velocity=False)
     threads = len(os.sched_getaffinity(0))
-    R, M = 8, 4
-    for _ in range(args.warmup):
-        cpu_baseline(m.H, m.n, threads, R, M)
-    times = [cpu_baseline(m.H, m.n, threads, R, M) for _ in range(args.steps)]
-    sec = sum(t["seconds"] for t in times) / len(times)
-    value = m.n * M * R / sec
-    cb = dict(times[0])
-    cb["value"] = value
-    cb.pop("seconds", None)
+    R, M = args.vectors, args.moments
+    B = np.exp(2j * np.pi * np.random.default_rng(9).random((m.n, R)))
+    c, a = (BOUNDS[0] + BOUNDS[1]) / 2, (BOUNDS[1] - BOUNDS[0]) / 2
+    eng = _ref_engine(m.H, sp.identity(m.n, format="csr"), threads)
+    kind = "reference"
+    if eng is not None:
+        run = lambda k: eng.core.moments(B, k, c, a)  # noqa: E731
+    else:
+        from oracle import kpm_oracle as O
+        oe = O.engine_from_model(m.H, sp.identity(m.n, format="csr"))
+        run = lambda k: oe.moments(B, k, c, a)  # noqa: E731
+        kind, threads = "port", 1
+    # warm-up steps are set-up calls (M=1); each timed step is one M=2 call
+    # (set-up + one operator application on all R vectors)
+    setups = []
+    for _ in range(max(args.warmup, 1)):
+        t0 = time.perf_counter()
+        run(1)
+        setups.append(time.perf_counter() - t0)
+    t_setup = min(setups)
+    apps = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        run(2)
+        apps.append(time.perf_counter() - t0 - t_setup)
+    t_app = max(statistics.median(apps), 1e-9)
+    full = t_setup + (M - 1) * t_app
+    value = m.n * M * R / full
+    cb = {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+          "applications_per_s": m.n * R / t_app, "seconds_per_application": t_app, "setup_seconds": t_setup,
+          "sample": f"Engine::moments on the full {m.n:,}-site lattice, R={R}: warm-up steps are M=1 calls "
+                    f"(set-up, min {t_setup:.2f} s), each timed step one M=2 call; the application time is its "
+                    f"median minus the set-up ({t_app:.2f} s), and the M={M} call is extrapolated as set-up + "
+                    f"{M - 1} applications ({threads} OpenMP threads)"}
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": full * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded lattice and phases)",
+            "applications_per_s": m.n * R / t_app,
             "config": {**config(args, m.n), "reference_sample": cb["sample"]}, "cpu_baseline": cb,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+class _RefOps:
+    """The compiled reference engine (oracle/_ref) behind the method names the
+    oracle's stepwise orchestration calls, counting operator applications
+    (moment steps of Engine::moments are direct: M - 1 per call)."""
+
+    def __init__(self, ref, S):
+        self.core, self.applications = ref.core, 0
+        self.metric = type("M", (), {"mul": staticmethod(lambda B: S @ B)})()
+
+    def moments(self, B, length, c, a):
+        self.applications += (length - 1) * B.shape[1]
+        return self.core.moments(B, length, c, a)
+
+    def series(self, B, coeff, c, a, directions=()):
+        self.applications += (len(coeff) - 1) * B.shape[1]
+        return self.core.series(B, coeff, c, a, directions)
+
+
+def _bench_call(fn, sync):
+    sync()
+    t0 = time.perf_counter()
+    out = fn()
+    sync()
+    return out, time.perf_counter() - t0
+
+
+def config_c1(threads):
+    """Config 1 in full: 64 x 64 square lattice, R=8, M=512, 201 energies,
+    stepwise MSD along x over 0-50 fs at dt = 1 fs, no VAC; FP64 and mixed,
+    moment doubling.  Work in the survey's unit: N per application of the
+    scaled operator to one vector (moment and propagation steps)."""
+    import torch
+    import scipy.sparse as sp
+    from kubomsd_b200 import kpm, lattices, stochastic
+    from kubomsd_b200.config import RunConfig
+    from kubomsd_b200.operators import build_operators
+    m = lattices.square_lattice(64)
+    B = kpm.random_phases(m.n, 20261019, range(8))
+    grid = dict(energy_eV=np.linspace(-11, 11, 201), spectral_bounds=(-11.2, 11.2), n_moments=512, axes=("x",),
+                include_vac=False, stochastic_method="stepwise")
+    out = {"workload": "config 1 in full: stepwise MSD, square 64x64 = 4,096 sites, R=8, M=512, 201 energies, "
+                       "0-50 fs at dt = 1 fs, x axis, no VAC", "unit": "orbital·moment·vec/s (N per operator "
+                                                                        "application to one vector)"}
+    res = {}
+    for prec in ("fp64", "mixed"):
+        cfg = RunConfig(time_fs=np.arange(51.), precision=prec, moment_doubling=True, **grid)
+        ops = build_operators(m, cfg)
+        stochastic.stepwise_samples(ops, cfg, B)
+        a0, l0 = ops.native.vector_applications, _launches()
+        (dos, nums, diag), dt = _bench_call(lambda: stochastic.stepwise_samples(ops, cfg, B), torch.cuda.synchronize)
+        apps = ops.native.vector_applications - a0
+        res[prec] = (dos, nums["msd_A2/commutator"])
+        out[prec] = {"seconds": dt, "value": m.n * apps / dt, "vector_applications": apps,
+                     "gpu_launches": _launches() - l0}
+    from kubomsd_b200 import accuracy
+    out["mixed_vs_fp64"] = accuracy.stepwise_errors(res["mixed"][0], res["mixed"][1], res["fp64"][0],
+                                                    res["fp64"][1], np.arange(51.))
+    out["value"] = out["mixed"]["value"]
+    # each launch is a few microseconds over a 512 KiB vector block: launch- and latency-bound
+    out["roofline"] = {"bound": "launch/latency (working set of 0.5-1 MiB per vector block, L2-resident)",
+                       "achieved": None, "peak": None, "frac": None}
+    ref = _ref_engine(m.H, m.S, threads, velocity=m.velocity)
+    if ref is not None:
+        from oracle import kpm_oracle as O
+        eng = _RefOps(ref, sp.identity(m.n, format="csr"))
+        t_end = 5.
+        _, dt = _bench_call(lambda: O.stepwise_samples(eng, B, grid["energy_eV"], np.arange(t_end + 1.),
+                                                        grid["spectral_bounds"], 512, [[1., 0., 0.]]), lambda: None)
+        out["cpu_baseline"] = {"value": m.n * eng.applications / dt, "unit": out["unit"], "cores": threads,
+                               "kind": "reference",
+                               "sample": f"the same stepwise run over 0-{t_end:g} fs (the reference's compiled "
+                                         f"Engine::moments / Engine::series driven by the oracle's restatement of "
+                                         f"stepwise.py), {eng.applications} vector applications in {dt:.2f} s"}
+    return out
+
+
+def config_c3_msd(threads, R=64, M=4096, t_end=5.):
+    """Config 3 stepwise MSD (the precision form's MSD(E, t)): honeycomb
+    4,194,304 sites with its explicit velocity, R=64 vectors, M=4096, x axis,
+    mixed form with moment doubling, over 0-t_end fs at dt = 1 fs (config 1's
+    grid, truncated to keep the bench short; the cost is linear in the number
+    of time points).  The augmented series step (MODE_SERIES: H, V and the
+    Bessel accumulation fused, [psi | phi] = 2R columns) is timed on its own
+    for its roofline."""
+    import torch
+    import scipy.sparse as sp
+    from kubomsd_b200 import kpm, lattices, stochastic
+    from kubomsd_b200.config import RunConfig
+    from kubomsd_b200.operators import build_operators
+    m = lattices.honeycomb(2048, 1024)
+    n = m.n
+    B = devstats_phases(n, 20261019, range(R))
+    cfg = RunConfig(energy_eV=np.linspace(-9, 9, 201), time_fs=np.arange(t_end + 1.), spectral_bounds=BOUNDS,
+                    n_moments=M, axes=("x",), include_vac=False, stochastic_method="stepwise", precision="mixed",
+                    moment_doubling=True)
+    ops = build_operators(m, cfg)
+    c, a = kpm.scaling(cfg)
+    out = {"workload": f"config 3 stepwise MSD: honeycomb {n:,} sites, R={R}, M={M}, 201 energies, 0-{t_end:g} fs "
+                       f"at dt = 1 fs, x axis, mixed, moment doubling", "unit": "orbital·moment·vec/s (N per operator "
+                                                                                  "application to one vector)"}
+    # the augmented series step alone: one 1 fs Bessel propagation of [psi | phi]
+    coeff, _ = kpm.bessel_coefficients(1., cfg, weighted_tail=True)
+    aug = torch.cat([B, torch.zeros_like(B)], dim=1).contiguous()
+    ops.native.series(aug, coeff, c, a, [[1., 0., 0.]])
+    l0 = _launches()
+    res, dt = _bench_call(lambda: ops.native.series(aug, coeff, c, a, [[1., 0., 0.]]), torch.cuda.synchronize)
+    steps = len(coeff) - 1
+    cols = 2 * R
+    row_bytes = 5 * cols * 8 + 4 * (4 + 4) + 3 * (4 + 8) + 8  # vectors (complex64) + H ELL row + V row
+    peak, src = peaks()
+    ach = n * row_bytes / (dt / steps) / 1e9
+    out["series_step"] = {"seconds_per_1fs_propagation": dt, "steps": steps, "ms_per_step": dt / steps * 1e3,
+                          "gpu_launches": _launches() - l0,
+                          "roofline": {"bound": "hbm", "kernel": "cheb_step_kernel MODE_SERIES (inline velocity)",
+                                       "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                       "peak_source": peak_src_note(src),
+                                       "algorithmic_bytes_per_row": row_bytes,
+                                       "timing": "propagation call time / Bessel steps (includes the set-up copies)"}}
+    del res, aug
+    a0 = ops.native.vector_applications
+    (dos, nums, diag), dt = _bench_call(lambda: stochastic.stepwise_samples(ops, cfg, B, device=True),
+                                        torch.cuda.synchronize)
+    apps = ops.native.vector_applications - a0
+    out.update(seconds=dt, value=n * apps / dt, vector_applications=apps)
+    del ops, dos, nums
+    torch.cuda.empty_cache()
+    ref = _ref_engine(m.H, m.S, threads, velocity=m.velocity)
+    if ref is not None:
+        Rc = 8
+        Bh = B[:, :Rc].cpu().numpy()
+        augh = np.concatenate([Bh, np.zeros_like(Bh)], axis=1)
+        cf = np.asarray(coeff[:2])
+        _, t2 = _bench_call(lambda: ref.core.series(augh, cf, c, a, [[1., 0., 0.]]), lambda: None)
+        _, t1 = _bench_call(lambda: ref.core.moments(Bh, 2, c, a), lambda: None)
+        out["cpu_baseline"] = {"value": n * 2 * Rc / t2, "unit": out["unit"], "cores": threads, "kind": "reference",
+                               "moments_application_per_s": n * Rc / t1,
+                               "sample": f"Engine::series of [psi | phi] ({2 * Rc} columns) with one Chebyshev term "
+                                         f"(one augmented application, {t2:.2f} s) and an M=2 Engine::moments call "
+                                         f"on R={Rc} ({t1:.2f} s), full lattice, {threads} OpenMP threads"}
+    return out
+
+
+def config_c2(threads, storage=("fp64", "mixed"), M=1024):
+    """Config 2 at full size: diamond sp3, 32,000 orbitals, kappa(S) = 50,
+    block-Jacobi batched PCG to rtol 1e-10 in every operator application,
+    R=32, M=1024 moments (direct: the general metric has no product identity)."""
+    import torch
+    import scipy.linalg as la
+    import scipy.sparse as sp
+    from types import SimpleNamespace
+    from kubomsd_b200 import kpm, lattices
+    from kubomsd_b200.native import B200Metric, B200Operators
+    m = lattices.diamond_sp3(cells=10)
+    S = sp.csr_matrix(m.S)
+    blocks = [(a, b, la.cholesky(S[a:b, a:b].toarray(), lower=True)) for a, b in m.atom_slices]
+    cfg = SimpleNamespace(metric_rtol=1e-10, metric_atol=0., metric_maxiter=1000, metric_residual_policy="fixed",
+                          metric_check_interval=32, metric_gap_ratio=.1, metric_solver="pcg", precision="fp64",
+                          moment_doubling=False)
+    R, c, a = 32, 0., 40.
+    B = torch.from_numpy(kpm.random_phases(m.n, 20261019, range(R))).cuda()
+    out = {"workload": f"config 2: KPM moments, diamond sp3 {m.n:,} orbitals, kappa(S)=50, block-Jacobi PCG "
+                       f"rtol 1e-10, R={R}, M={M}", "unit": UNIT}
+    for st in storage:
+        metric = B200Metric(S, S.diagonal().real.copy(), blocks, cfg)
+        metric.set_storage(st)
+        eng = B200Operators(SimpleNamespace(host_H=m.H, metric=SimpleNamespace(native=metric), velocity={},
+                                            position={}, composite={}), cfg)
+        eng.moments(B, 8, c, a)
+        s0, l0 = metric.stats(), _launches()
+        _, dt = _bench_call(lambda: eng.moments(B, M, c, a), torch.cuda.synchronize)
+        s1 = metric.stats()
+        iters = s1.max_iterations_sum - s0.max_iterations_sum
+        solves = s1.calls - s0.calls
+        vec = m.n * R * (16 if st == "fp64" else 8)
+        # per PCG iteration: S p (read p, write Sp), update (read p, Sp, y, r; write y, r, z; y is complex128),
+        # direction (read z, p; write p), and the 4x4-block S values and indices once
+        s_bytes = S.nnz * 8 + S.nnz // 16 * 4
+        it_bytes = 11 * vec + 2 * m.n * R * 16 + s_bytes
+        out[f"storage_{st}"] = {"seconds": dt, "value": m.n * M * R / dt, "applications_per_s": m.n * R * (M - 1) / dt,
+                                "metric_solves": solves, "pcg_iterations_per_solve": iters / max(solves, 1),
+                                "us_per_pcg_iteration": dt / max(iters, 1) * 1e6, "gpu_launches": _launches() - l0,
+                                "bytes_per_pcg_iteration": it_bytes}
+        del eng, metric
+        torch.cuda.empty_cache()
+    best = min((k for k in out if k.startswith("storage_")), key=lambda k: out[k]["seconds"])
+    out["value"] = out[best]["value"]
+    peak, src = peaks()
+    ach = out[best]["bytes_per_pcg_iteration"] / (out[best]["us_per_pcg_iteration"] * 1e-6) / 1e9
+    out["roofline"] = {"bound": "L2/latency: the PCG working set (seven 16 MB vector blocks, 17 MB of S) is "
+                                "L2-resident, so the HBM figure below is for information",
+                       "kernel": "PCG iteration (pcg_spmv + pcg_update + pcg_direction)", "achieved": ach,
+                       "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_source": peak_src_note(src),
+                       "algorithmic_bytes_per_iteration": out[best]["bytes_per_pcg_iteration"]}
+    ref = _ref_engine(m.H, S, threads, blocks=[(a0, b0, L) for a0, b0, L in blocks])
+    if ref is not None:
+        Bh = B.cpu().numpy()
+        t_setup, t_app, _ = time_applications(lambda k: ref.core.moments(Bh, k, c, a))
+        full = t_setup + (M - 1) * t_app
+        out["cpu_baseline"] = {"value": m.n * M * R / full, "unit": UNIT, "cores": threads, "kind": "reference",
+                               "applications_per_s": m.n * R / t_app,
+                               "sample": f"Engine::moments on the full model, R={R}: one M=1 call (S B, "
+                                         f"{t_setup:.2f} s) and one M=2 call (one H product + one PCG solve, "
+                                         f"{t_app:.2f} s); M={M} extrapolated as set-up + {M - 1} applications"}
+    return out
+
+
+def config_c5(duration=8., rate=20., msd_fraction=.25):
+    """Config 5 (a sampled window): Poisson arrivals at 20 req/s of DOS and
+    stepwise-MSD jobs over resident orthogonal lattices (16k-4M sites) and
+    nonorthogonal sp3 cells, M in {512, 1024, 2048}, R in {8, 32}, admitted by
+    an HBM budget of 150 GB into 8 slots; p50/p99 latency and throughput."""
+    from kubomsd_b200 import lattices
+    from kubomsd_b200.serving import ResidentModel, Server, latency_summary, poisson_stream
+    models = {
+        "sq128": ResidentModel("sq128", lattices.square_lattice(128, seed=1), (-11.5, 11.5), replicas=8),
+        "hc1024": ResidentModel("hc1024", lattices.honeycomb(1024, 512, seed=2), (-9.2, 9.2), replicas=8),
+        "hc2048": ResidentModel("hc2048", lattices.honeycomb(2048, 1024, seed=3), (-9.2, 9.2), replicas=8),
+        "sp3_8k": ResidentModel("sp3_8k", lattices.diamond_sp3(cells=4), (-40., 40.), precision="fp64",
+                                replicas=8),
+    }
+    reqs = poisson_stream(rate, duration, models, seed=5, msd_fraction=msd_fraction, times_fs=(0., 1., 2.))
+    srv = Server(models, slots=8, hbm_budget_bytes=150 * 10 ** 9)
+    t0 = time.perf_counter()
+    res = srv.serve(reqs)
+    wall = time.perf_counter() - t0
+    busy = sum(r.end - r.start for r in res)
+    return {"workload": f"serving: Poisson {rate:g} req/s for a {duration:g} s window, {msd_fraction:.0%} stepwise "
+                        "MSD jobs (x axis, 0/1/2 fs) and DOS jobs, M in {512,1024,2048}, R in {8,32}, models "
+                        + ", ".join(f"{k} ({mm.n:,} orbitals)" for k, mm in models.items())
+                        + ", 8 slots, HBM budget 150 GB",
+            "latency": latency_summary(res), "requests": len(res), "errors": len(srv.errors),
+            "jobs": {"dos": sum(r.kind == "dos" for r in res), "msd": sum(r.kind == "msd" for r in res)},
+            "wall_s": wall, "requests_per_s": len(res) / wall, "offered_rate": rate,
+            "slot_occupancy": busy / (8 * wall)}
+
+
+def devstats_phases(n, seed, ids):
+    from kubomsd_b200 import devstats
+    return devstats.random_phases(n, seed, ids)
+
+
+def _launches():
+    from kubomsd_b200 import _abi
+    return int(_abi.require_library().kmsd_kernel_launches())
+
+
+def peak_src_note(src):
+    return f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else src
 
 
 def run_diamond(args):
@@ -381,9 +690,10 @@ def main():
     m = lattices.honeycomb(args.lx, args.ly, with_velocity=False)
     n, R, M = m.n, args.vectors, args.moments
     # this rank's statistics block: sample ids rank*R .. rank*R+R-1
+    from kubomsd_b200 import devstats
+    B = devstats.random_phases(n, 20261019, range(rank * R, rank * R + R))  # NumPy's PCG64 stream, on the device
     host = torch.empty((n, R), dtype=torch.complex128, pin_memory=True)
-    host.numpy()[:] = kpm.random_phases(n, 20261019, range(rank * R, rank * R + R))
-    B = host.to("cuda", non_blocking=False)
+    host.copy_(B)
     c, a = (BOUNDS[0] + BOUNDS[1]) / 2, (BOUNDS[1] - BOUNDS[0]) / 2
 
     def engine(precision, method):
@@ -443,7 +753,12 @@ def main():
             "bytes_per_omv": bytes_per_launch / (n * R * (2 if args.method == "doubling" else 1)),
             "timing": "step time / launches per step (includes the 3 small set-up kernels of each step)"}
 
+    apps_per_step = launches_per_step * R  # one operator application per step launch and column
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "applications_per_s": world * n * apps_per_step / (ms_step / 1e3),
+            "value_counts": "moments: N*M*R per moments call; under the product identity each operator "
+                            "application yields two moments, so applications_per_s (one application of the scaled "
+                            "operator to one length-N vector = N) is value/2",
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64 vectors / f64 accumulation" if args.precision == "mixed" else "c128",
             "data": "synthetic (seeded honeycomb lattice, NumPy PCG64 random phases)",
@@ -503,7 +818,18 @@ def main():
         except Exception as exc:  # noqa: BLE001 - reported, not fatal to the timing line
             line["msd_check"] = {"error": f"{type(exc).__name__}: {exc}"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(m.H, n, len(os.sched_getaffinity(0)))
+        line["cpu_baseline"] = cpu_baseline(m.H, n, len(os.sched_getaffinity(0)), R, M)
+    if rank == 0 and world == 1 and not args.no_configs:
+        threads = len(os.sched_getaffinity(0))
+        configs = {}
+        for name, fn in (("c1", lambda: config_c1(threads)), ("c2", lambda: config_c2(threads)),
+                         ("c3_msd", lambda: config_c3_msd(threads)), ("c5", config_c5)):
+            try:
+                configs[name] = fn()
+            except Exception as exc:  # noqa: BLE001 - reported, not fatal to the headline line
+                configs[name] = {"error": f"{type(exc).__name__}: {exc}"}
+            torch.cuda.empty_cache()
+        line["configs"] = configs
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -237,6 +237,70 @@ int kmsd_engine_series(kmsd_engine e, const void *b_in, void *out, int64_t b,
 int kmsd_engine_chain(kmsd_engine e, const void *b_in, void *out, int64_t b,
                       int64_t length, double center, double half, void *stream);
 
+/* The correlation tables of the spectral VAC without storing the chain:
+ * tables[c, j, k] = sum_n conj(T_j(Ht) B)[n, c] * cov[n, k, c]
+ * for j < length, k < kcols and column c < b, written as a (b, length, kcols)
+ * complex128 device array (tables[(c*length + j)*kcols + k]).  cov is the
+ * (n, kcols, b) complex128 device array of the velocity applied to the right
+ * chain T_k(Ht) v.  Replaces the reference's stored left chain
+ * (Engine::chain, cpp/native.cpp:574-589) followed by the contraction
+ * `np.einsum` of src/kubo_msd/solvers/spectral.py:33-38: the chain is
+ * generated into a ring of 32 vector blocks and contracted as it goes.
+ * b <= 8 and kcols <= 1024 / b per call. */
+int kmsd_engine_chain_correlate(kmsd_engine e, const void *b_in, const void *cov,
+                                int64_t b, int64_t length, int64_t kcols,
+                                double center, double half, void *tables,
+                                void *stream);
+
+/* The per-node tail of the spectral VAC (src/kubo_msd/solvers/spectral.py:
+ * 39-51) for `nodes` time nodes at once, on the device: with Bessel
+ * coefficients coeff[m][p] (complex128, (nodes, kcols), device; p <= orders[m],
+ * orders an int32 device array) and tables from
+ * kmsd_engine_chain_correlate,
+ *   q[m][c][j]   = sum_k tables[c][j][k] coeff[m][k],
+ *   mom[m][c][l] = Re sum_p (q[m][c][l+p] + q[m][c][|l-p|]) / 2 conj(coeff[m][p]),
+ *   vac[m][c][e] = sum_l G[e][l] mom[m][c][l]   (l < n_moments),
+ * with G the (n_energy, n_moments) reconstruction matrix (float64, device)
+ * and vac a (nodes, b, n_energy) float64 device array.  `work` is device
+ * scratch of at least nodes*b*(16*length + 8*n_moments) bytes.  Asynchronous. */
+/* The reference sampler's random phases on the device: out[r*b + c] =
+ * exp(2 pi i u_rc), u_rc the r-th double of NumPy's
+ * Generator(PCG64(SeedSequence([seed, id_c]))).random(n)
+ * (src/kubo_msd/metric/sampling.py:8-9).  pcg_state is a device array of b x
+ * 4 uint64: each column's PCG64 state (low, high 64 bits) and increment (low,
+ * high) as SeedSequence sets them up.  The u are bit-identical to NumPy's;
+ * the phases agree to a few ulp (device sincos).  out is (n, b) complex128 on
+ * the device.  Asynchronous. */
+int kmsd_random_phases(int64_t n, int64_t b, const uint64_t *pcg_state,
+                       void *out, void *stream);
+
+/* out[c*n_energy + e] = sum_l G[e*length + l] mu[l*b + c]: the projection
+ * (G mu)^T of moments onto the energy grid (src/kubo_msd/solvers/
+ * chebyshev.py:50-54), all arrays float64 on the device.  Asynchronous. */
+int kmsd_project_moments(const double *mu, int64_t length, int64_t b,
+                         const double *G, int64_t n_energy, double *out,
+                         void *stream);
+
+/* Paired block bootstrap of a ratio of block sums on the device
+ * (src/kubo_msd/observables/statistics.py:5-23; the reference's device form
+ * kubo_msd_gpu/src/kubo_msd/observables/statistics_gpu.py:6-28): A is the
+ * (nblocks, P) block numerators and D the (nblocks, n_energy) block
+ * denominators, broadcast over P = (...) x n_energy; value[p] = sum A / sum D
+ * (NaN where the sum of D is zero) and, when stderr_out is not NULL,
+ * stderr_out[p] = standard deviation (ddof 1) over the n_resamples rows of
+ * `weights` (nres, nblocks; the count of each block in each resample, drawn
+ * by the caller) of the resampled ratios.  Float64 device arrays.
+ * Asynchronous. */
+int kmsd_bootstrap_ratio(const double *A, const double *D, int64_t nblocks,
+                         int64_t P, int64_t n_energy, const double *weights,
+                         int64_t n_resamples, double *value, double *stderr_out,
+                         void *stream);
+
+int kmsd_vac_nodes(const void *tables, int64_t b, int64_t length, int64_t kcols,
+                   int64_t n_moments, const void *coeff, const int *orders,
+                   int64_t nodes, const double *G, int64_t n_energy, void *work,
+                   int64_t work_bytes, double *vac, void *stream);
+
 /* mu[k*b + j] = Re sum_i conj((S B)_ij) (T_k(Ht) B)_ij for k < length, on the
  * device (float64, (length, b)).  Engine::moments (cpp/native.cpp:590-609).
  * flags: KMSD_MOMENTS_DIRECT or KMSD_MOMENTS_DOUBLING (S = I only). */
@@ -253,10 +317,14 @@ int kmsd_engine_moments(kmsd_engine e, const void *b_in, double *mu, int64_t b,
  * MIXED once an allocating call has created the complex64 copy of H.  The
  * workspace is one static 64 MiB device block per GPU (part of the library
  * image, held until exit); calls that need more are rejected with
- * KMSD_EINVAL.  The first call on a GPU looks up the block's address; make it
- * before any stream capture.  All calls on a GPU share the block: calls that
- * overlap on the GPU race, so keep them on one stream.  Asynchronous on
- * `stream`; mu is device memory (length, b). */
+ * KMSD_EINVAL.  Under CUDA's lazy module loading (the default) the block is
+ * reserved at the first call on each GPU, which may then synchronise or fail
+ * with out-of-memory: callers that need the no-stall, no-out-of-memory
+ * promise make one warm-up call per GPU at start-up.  The first call in a
+ * CUDA context also looks up the block's address; make it before any stream
+ * capture.  No handle survives cudaDeviceReset.  All calls on a GPU share the
+ * block: calls that overlap on the GPU race, so keep them on one stream.
+ * Asynchronous on `stream`; mu is device memory (length, b). */
 int kmsd_engine_moments_noalloc(kmsd_engine e, const void *b_in, double *mu,
                                 int64_t b, int64_t length, double center,
                                 double half, int flags, void *stream);
@@ -324,6 +392,10 @@ int kmsd_batch_rows(kmsd_batch bt, int64_t *offsets);
 int kmsd_batch_moments(kmsd_batch bt, const void *b_in, double *mu, int64_t b,
                        int64_t length, const double *center, const double *half,
                        int flags, int use_graph, void *stream);
+
+/* Sets the row-tile size of the batch step kernels (as chosen by
+ * kmsd_batch_tune).  No counterpart in the reference. */
+int kmsd_batch_set_tile_rows(kmsd_batch bt, int64_t tile_rows);
 
 /* Autotuner: times the tile sizes 512..8192 rows on this call's shape and
  * keeps the fastest (written to *chosen_tile_rows). */

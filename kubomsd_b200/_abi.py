@@ -68,6 +68,11 @@ SIGNATURES = {
     "kmsd_engine_v_cov": (C.c_int, [P, PD, P, P, I64, D, D, C.c_int, P]),
     "kmsd_engine_series": (C.c_int, [P, P, P, I64, PD, I64, D, D, PD, I64, P]),
     "kmsd_engine_chain": (C.c_int, [P, P, P, I64, I64, D, D, P]),
+    "kmsd_engine_chain_correlate": (C.c_int, [P, P, P, I64, I64, I64, D, D, P, P]),
+    "kmsd_vac_nodes": (C.c_int, [P, I64, I64, I64, I64, P, P, I64, P, I64, P, I64, P, P]),
+    "kmsd_random_phases": (C.c_int, [I64, I64, P, P, P]),
+    "kmsd_project_moments": (C.c_int, [P, I64, I64, P, I64, P, P]),
+    "kmsd_bootstrap_ratio": (C.c_int, [P, P, I64, I64, I64, P, I64, P, P, P]),
     "kmsd_engine_moments": (C.c_int, [P, P, PD, I64, I64, D, D, C.c_int, P]),
     "kmsd_engine_moments_noalloc": (C.c_int, [P, P, PD, I64, I64, D, D, C.c_int, P]),
     "kmsd_engine_counters": (C.c_int, [P, PI64, PI64]),
@@ -79,6 +84,7 @@ SIGNATURES = {
     "kmsd_batch_destroy": (None, [P]),
     "kmsd_batch_rows": (C.c_int, [P, PI64]),
     "kmsd_batch_moments": (C.c_int, [P, P, PD, I64, I64, PD, PD, C.c_int, C.c_int, P]),
+    "kmsd_batch_set_tile_rows": (C.c_int, [P, I64]),
     "kmsd_batch_tune": (C.c_int, [P, P, PD, I64, I64, PD, PD, C.c_int, PI64, P]),
 }
 

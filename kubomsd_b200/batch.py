@@ -87,13 +87,25 @@ class B200Batch:
                  for b in blocks]
         return torch.cat([p.to("cuda", torch.complex128) for p in parts], dim=0).contiguous()
 
+    col_block = 0  # vector-block width of one batch call (0: all columns), set by tune()
+
     def moments(self, B, length, centers, halves, doubling=True, use_graph=True):
-        """(ninst, length, b) float64 device tensor of Jackson-KPM moments."""
+        """(ninst, length, b) float64 device tensor of Jackson-KPM moments; the
+        columns run in blocks of `col_block` vectors when tune() chose that."""
         torch = _torch()
         if isinstance(B, (list, tuple)):
             B = self.concat(B)
         if B.shape[0] != self.n:
             raise ValueError("batch block rows must equal the sum of instance sizes")
+        w = self.col_block
+        if w and w < B.shape[1]:
+            parts = [self._moments_block(B[:, j0:j0 + w].contiguous(), length, centers, halves, doubling, use_graph)
+                     for j0 in range(0, B.shape[1], w)]
+            return torch.cat(parts, dim=2)
+        return self._moments_block(B, length, centers, halves, doubling, use_graph)
+
+    def _moments_block(self, B, length, centers, halves, doubling, use_graph):
+        torch = _torch()
         b = B.shape[1]
         c = np.ascontiguousarray(np.broadcast_to(np.asarray(centers, float), (self.ninst,)))
         h = np.ascontiguousarray(np.broadcast_to(np.asarray(halves, float), (self.ninst,)))
@@ -112,9 +124,38 @@ class B200Batch:
         return mu.clone()
 
     def tune(self, B, length, centers, halves, doubling=True):
+        """Autotunes the row-tile size and the vector-block width: for each
+        width (all columns, half, a quarter; even widths in the mixed form)
+        the library sweeps the tile sizes, then whole calls with that width
+        and its best tile are timed.  Keeps the fastest pair; returns the tile
+        rows (the width is in `col_block`)."""
         torch = _torch()
         if isinstance(B, (list, tuple)):
             B = self.concat(B)
+        b = B.shape[1]
+        widths = [w for w in (b, b // 2, b // 4) if w >= 1 and b % w == 0 and
+                  (self.precision != "mixed" or w % 2 == 0)]
+        best = None
+        for w in dict.fromkeys(widths):
+            rows = self._tune_rows(B[:, :w].contiguous(), length, centers, halves, doubling)
+            self.col_block = w
+            self.moments(B, length, centers, halves, doubling)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            self.moments(B, length, centers, halves, doubling)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            if best is None or ms < best[0]:
+                best = (ms, w, rows)
+        _, self.col_block, rows = best
+        _check(self.lib, self.lib.kmsd_batch_set_tile_rows(self.handle, int(rows)))
+        self.tuned = {"tile_rows": rows, "col_block": self.col_block, "ms": best[0]}
+        return rows
+
+    def _tune_rows(self, B, length, centers, halves, doubling):
+        torch = _torch()
         b = B.shape[1]
         c = np.ascontiguousarray(np.broadcast_to(np.asarray(centers, float), (self.ninst,)))
         h = np.ascontiguousarray(np.broadcast_to(np.asarray(halves, float), (self.ninst,)))

@@ -22,7 +22,7 @@ LIBNAME = "libkmsd_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-Xcompiler", "-Wall", "-Xcompiler", "-Wno-unused-function"]
-SOURCES = ["kmsd_engine.cu", "kmsd_metric.cu", "kmsd_ops.cu", "kmsd_noalloc.cu", "kmsd_batch.cu"]
+SOURCES = ["kmsd_engine.cu", "kmsd_metric.cu", "kmsd_ops.cu", "kmsd_noalloc.cu", "kmsd_batch.cu", "kmsd_corr.cu", "kmsd_stats.cu"]
 
 
 def nvcc() -> str:

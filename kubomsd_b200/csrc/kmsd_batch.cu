@@ -750,6 +750,11 @@ int kmsd_batch_moments(kmsd_batch bt, const void *b_in, double *mu, int64_t b, i
                       use_graph != 0);
 }
 
+int kmsd_batch_set_tile_rows(kmsd_batch bt, int64_t tile_rows) {
+    if (!bt || tile_rows < 1) return fail(KMSD_EINVAL, "invalid batch");
+    return build_tiles(bt, tile_rows);
+}
+
 int kmsd_batch_tune(kmsd_batch bt, const void *b_in, double *mu, int64_t b, int64_t length, const double *center,
                     const double *half, int flags, int64_t *chosen_tile_rows, void *stream) {
     if (!bt) return fail(KMSD_EINVAL, "invalid batch");

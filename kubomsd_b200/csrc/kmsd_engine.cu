@@ -370,6 +370,9 @@ int kmsd_csr_create(int64_t n, const int64_t *indptr, const int64_t *indices, co
     A->nnz = nnz;
     A->complex_values = cplx;
     A->identity = ident;
+    bool diag = nnz == n && !cplx;
+    for (int64_t r = 0; r < n && diag; ++r) diag = indptr[r] == r && indices[r] == r;
+    A->diagonal = diag;
     cudaGetDevice(&A->device);
     auto up = [&](void **dst, const void *src, size_t bytes) -> int {
         KMSD_CUDA(cudaMalloc(dst, std::max<size_t>(bytes, 16)));

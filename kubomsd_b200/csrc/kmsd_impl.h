@@ -69,6 +69,9 @@ struct kmsd_csr_s {
     float *re32 = nullptr, *im32 = nullptr;  // created on first mixed use
     bool complex_values = false;
     bool identity = false;
+    // one real entry per row, on the diagonal (a position operator given by
+    // site coordinates): re64 then holds the coordinates in row order
+    bool diagonal = false;
     int device = 0;
     // ELL copy for short rows (see EllView); ell_w == 0 when not built.
     int ell_w = 0;
@@ -102,6 +105,10 @@ int take_real(const double2 *src, double *dst, int64_t b, cudaStream_t s);
 // y = sum coef_m x_m  (or y += ...).
 int lincomb(cudaStream_t s, double2 *y, int64_t len, int accumulate, int terms, const double2 *const *x,
             const double *cr, const double *ci);
+// Correlation tables of ring slots [j0, j0 + jn) against cov (kmsd_corr.cu).
+int corr_ring(const double2 *ring, int64_t n, int nb, const double2 *cov, int k1, int64_t j0, int jn,
+              int64_t length, double2 *tables, DevBuf &partial, cudaStream_t s);
+int ring_slots();
 // Shared scratch for reductions (partials + tickets), grown per call site.
 struct Reducer {
     DevBuf partial;
@@ -211,6 +218,7 @@ struct kmsd_engine_s {
     int64_t h_calls = 0, v_calls = 0;
     bool identity = false;
     kmsd::DevBuf ta, tb, bra, hx, t1, t2, t3, t4, t5, psi, vc, inj[3], outw;
+    kmsd::DevBuf ring, corr_partial;  // left-chain ring and partial sums of the correlation tables
     kmsd::DevBuf status;  // int[4]: [0] code, [1] report claim, [2] series nonfinite
     kmsd::DevBuf report;  // FailReportFull
     kmsd::DevBuf dots;    // double2[512]

@@ -238,6 +238,26 @@ __device__ __forceinline__ Pk<T> gather_unit(const CsrView<T> &A, const typename
     return acc;
 }
 
+// sum_j H_ij (x_j - x_i) X[j, unit u]: the commutator [H, X] with the
+// diagonal X = diag(x) applied to one unit of the row, from H's CSR row.
+// The coordinate difference is formed in FP64 before it meets H_ij, so
+// large absolute coordinates lose no precision in the mixed form.
+template <class T>
+__device__ __forceinline__ Pk<T> gather_commutator(const CsrView<T> &A, const double *x,
+                                                   const typename Unit<T>::vec *X, int64_t row, int U, int u) {
+    Pk<T> acc = pk_zero<T>();
+    const int k0 = __ldg(A.ptr + row), k1 = __ldg(A.ptr + row + 1);
+    const double xi = __ldg(x + row);
+    for (int k = k0; k < k1; ++k) {
+        const int col = __ldg(A.idx + k);
+        const T d = (T)(__ldg(x + col) - xi);
+        const Pk<T> xv = ldg(X + (size_t)col * U + u);
+        if (A.im == nullptr) cmac_real(acc, d * __ldg(A.re + k), xv);
+        else cmac_cplx(acc, d * __ldg(A.re + k), d * __ldg(A.im + k), xv);
+    }
+    return acc;
+}
+
 // ------------------------------------------------------------ SpMM
 // Y = A X (optionally with per-column partial sums of conj(X_row) * Y_row,
 // the curvature <p, S p> of the metric solve).
@@ -324,8 +344,13 @@ template <class T> struct StepArgs {
     T c0r, c0i, ckr, cki;  // coefficients (c0 used when first)
     int UR;                // units of the psi block (0: no augmentation)
     int nphi;              // number of phi blocks
-    // inline velocity: for each axis, CSR and weight w[a][axis] (complex)
+    // inline velocity: for each axis, CSR and weight w[a][axis] (complex).
+    // vform[v] = 0: Vm[v] is the velocity matrix; 1: the velocity is the
+    // commutator i [H, X] / hbar with X = diag(xdiag[v]), applied from H's
+    // row (the i / hbar is folded into the weights)
     CsrView<T> Vm[3];
+    int vform[3];
+    const double *xdiag[3];
     int nvel;              // number of velocity matrices in use
     int vel_axis[3];
     T wr[4][3], wi[4][3];  // injection weights per phi block and velocity matrix
@@ -514,7 +539,8 @@ __global__ void __launch_bounds__(256, (step_pairs<MU, MODE, HSRC>() ? KMSD_STEP
                     for (int v = 0; v < a.nvel; ++v) {
                         const T wr = a.wr[blk][v], wi = a.wi[blk][v];
                         if (wr == T(0) && wi == T(0)) continue;
-                        const Pk<T> vp = gather_unit<T>(a.Vm[v], a.curr, row, mp.U, upsi);
+                        const Pk<T> vp = a.vform[v] ? gather_commutator<T>(a.H, a.xdiag[v], a.curr, row, mp.U, upsi)
+                                                    : gather_unit<T>(a.Vm[v], a.curr, row, mp.U, upsi);
 #pragma unroll
                         for (int c = 0; c < C; ++c) {
                             t.re[c] += wr * vp.re[c] - wi * vp.im[c];

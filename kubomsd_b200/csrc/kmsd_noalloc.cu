@@ -12,13 +12,19 @@
 // reduction ticket all live in `g_moments_scratch` below.
 //
 // Properties a caller must know:
-//  * the block is 64 MiB per GPU, allocated when the library's module is
-//    loaded on that GPU and held until the process exits;
+//  * the block is 64 MiB per GPU and is held until the process exits.  It is
+//    reserved when the runtime loads the library's device code on that GPU.
+//    Under CUDA's lazy module loading (the default since CUDA 12) that
+//    happens at the first call on each GPU, and that first call may then
+//    synchronise the device or fail with out-of-memory.  Callers that rely on
+//    "no stall, no out-of-memory" make one warm-up call per GPU at start-up;
 //  * calls whose buffers would not fit are rejected with KMSD_EINVAL and a
 //    message naming the bytes needed; kmsd_engine_moments has no such limit;
-//  * the first call on each GPU looks up the block's device address (once
-//    per device, under a lock); make that first call before any stream
-//    capture;
+//  * the block's device address is looked up with cudaGetSymbolAddress the
+//    first time a CUDA context calls (once per context, under a lock) and is
+//    cached per context.  Make that first call before any stream capture.
+//    cudaDeviceReset invalidates the cache together with every engine handle,
+//    whose device buffers the reset frees: no handle is usable after a reset;
 //  * every call on a GPU uses the same block and leaves its contents
 //    behind.  The call clears what must start at zero, so the contents left by
 //    an earlier call are harmless.  Two calls that overlap on the GPU, on
@@ -32,6 +38,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 
 #include "kmsd.h"
@@ -46,25 +53,52 @@ static __device__ __align__(256) unsigned char g_moments_scratch[kMomentsScratch
 
 namespace {
 
-constexpr int kMaxDevices = 64;
 std::mutex g_scratch_lock;
-void *g_scratch_address[kMaxDevices] = {};
+std::map<void *, void *> g_scratch_address;  // CUDA context -> device address of the block
 
-// Device address of g_moments_scratch on the current device.  In host code the
-// symbol names a host-side stand-in, not device memory, so its address is
-// looked up with cudaGetSymbolAddress once per device and cached.
+// The current CUDA context, or null when none is current on this thread (the
+// driver's cuCtxGetCurrent, reached through the runtime so the library needs
+// no link-time dependency on libcuda).
+int current_context(void **ctx) {
+    using GetCurrent = int (*)(void **);
+    static GetCurrent fn = nullptr;
+    if (fn == nullptr) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        KMSD_CUDA(cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || p == nullptr)
+            return fail(KMSD_ECUDA, "cuCtxGetCurrent is not available from the driver");
+        fn = reinterpret_cast<GetCurrent>(p);
+    }
+    *ctx = nullptr;
+    if (fn(ctx) != 0) return fail(KMSD_ECUDA, "cuCtxGetCurrent failed");
+    return KMSD_OK;
+}
+
+// Device address of g_moments_scratch in the current context.  In host code
+// the symbol names a host-side stand-in, not device memory, so its address is
+// looked up with cudaGetSymbolAddress once per context and cached.
 int scratch_address(void **out) {
-    int dev = 0;
-    KMSD_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return fail(KMSD_EINVAL, "device ordinal out of range for the moments scratch");
+    void *ctx = nullptr;
+    if (int rc = current_context(&ctx)) return rc;
+    if (ctx == nullptr) {
+        // no context current on this thread yet: make the current device's
+        // primary context current, as the runtime would on its first call
+        int dev = 0;
+        KMSD_CUDA(cudaGetDevice(&dev));
+        KMSD_CUDA(cudaSetDevice(dev));
+        if (int rc = current_context(&ctx)) return rc;
+        if (ctx == nullptr) return fail(KMSD_ECUDA, "no current CUDA context for the moments scratch");
+    }
     std::lock_guard<std::mutex> guard(g_scratch_lock);
-    if (g_scratch_address[dev] == nullptr) {
+    auto it = g_scratch_address.find(ctx);
+    if (it == g_scratch_address.end()) {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_moments_scratch);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_moments_scratch)");
-        g_scratch_address[dev] = p;
+        it = g_scratch_address.emplace(ctx, p).first;
     }
-    *out = g_scratch_address[dev];
+    *out = it->second;
     return KMSD_OK;
 }
 

@@ -466,6 +466,77 @@ int chain_impl(E *e, const double2 *B, double2 *out, int64_t b, int64_t len, dou
     return KMSD_OK;
 }
 
+// ---------------------------------------------------------------- correlate
+// tables[b, j, k] = <T_j(Ht) B[:, b], cov[:, k, b]> for j < len, k < k1,
+// with the chain generated into a ring of ring_slots() vector blocks and
+// contracted every ring_slots() steps (kmsd_corr.cu), never stored whole.
+// Step k writes slot k % J, which held T_{k-J}: the contraction that read it
+// was queued on the same stream before this step.
+int correlate_impl(E *e, const double2 *B, const double2 *cov, int64_t b, int64_t len, int64_t k1, double center,
+                   double half, double2 *tables, cudaStream_t s) {
+    const int64_t n = e->H->n;
+    const int64_t slab = n * b;
+    const int J = ring_slots();
+    const Ctl c{e->rtol, e->atol, e->maxiter};
+    if (ensure_vec(e->ring, n, b * J)) return KMSD_ECUDA;
+    double2 *ring = e->ring.as<double2>();
+    auto slot = [&](int64_t k) { return ring + (k % J) * slab; };
+    int rc;
+    auto contract_after = [&](int64_t k) -> int {  // chain index k was just written
+        if ((k + 1) % J != 0 && k != len - 1) return KMSD_OK;
+        const int64_t j0 = k - k % J;
+        return corr_ring(ring, n, (int)b, cov, (int)k1, j0, (int)(k - j0 + 1), len, tables, e->corr_partial, s);
+    };
+    KMSD_CUDA(cudaMemcpyAsync(slot(0), B, slab * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    if ((rc = contract_after(0))) return rc;
+    if (len == 1) return KMSD_OK;
+    if (e->precision == KMSD_FP64) {
+        StepArgs<double> a = base_args<double>(e, (int)b, center, half);
+        if (!e->identity) {
+            if (ensure_vec(e->hx, n, b)) return KMSD_ECUDA;
+            a.hx = e->hx.as<double2>();
+        }
+        for (int64_t k = 1; k < len; ++k) {
+            a.curr = slot(k - 1);
+            a.prev = k >= 2 ? slot(k - 2) : nullptr;
+            a.next = slot(k);
+            a.first = k == 1;
+            if (e->identity) {
+                ++e->h_calls;
+                if ((rc = launch_step<double, MODE_CHAIN, true, false>(e, a, s))) return rc;
+            } else {
+                if ((rc = h_action(e, a.curr, e->hx.as<double2>(), b, c, s))) return rc;
+                if ((rc = launch_step<double, MODE_CHAIN, false, false>(e, a, s))) return rc;
+            }
+            if ((rc = contract_after(k))) return rc;
+        }
+        return KMSD_OK;
+    }
+    if (!e->identity) return fail(KMSD_EINVAL, "mixed precision requires an identity metric (orthogonal basis)");
+    if (b % 2) return fail(KMSD_EINVAL, "mixed-precision chain needs an even number of columns");
+    const int U = (int)(b / 2);
+    if (ensure_vec(e->ta, n, U, sizeof(float4)) || ensure_vec(e->tb, n, U, sizeof(float4)) || e->H->ensure_f32())
+        return KMSD_ECUDA;
+    float4 *ta = e->ta.as<float4>(), *tb = e->tb.as<float4>();
+    if ((rc = to_f32(B, tb, n, b, U, s))) return rc;
+    StepArgs<float> a = base_args<float>(e, U, center, half);
+    float4 *curr = tb, *prev = nullptr;
+    for (int64_t k = 1; k < len; ++k) {
+        float4 *next = k == 1 ? ta : prev;
+        a.curr = curr;
+        a.prev = prev;
+        a.next = next;
+        a.first = k == 1;
+        a.store64 = slot(k);
+        if ((rc = launch_step<float, MODE_CHAIN, true, false>(e, a, s))) return rc;
+        if ((rc = contract_after(k))) return rc;
+        prev = curr;
+        curr = next;
+    }
+    e->h_calls += len - 1;
+    return KMSD_OK;
+}
+
 // ---------------------------------------------------------------- series
 struct Aug {
     int64_t nb = 0, ndir = 0;
@@ -474,14 +545,22 @@ struct Aug {
     int nvel = 0, vel_axis[3] = {0, 0, 0};
 };
 
-// Is every velocity contribution an explicit matrix (kind 0)?
+// Position operator of axis x given by site coordinates (a diagonal X) on an
+// orthogonal basis: its velocity i [H, X] / hbar is applied inside the step
+// kernel from H's rows.
+bool commutator_inline(const E *e, int x) {
+    return e->vel_kind[x] == 1 && e->identity && e->vel[3 * x] && e->vel[3 * x]->diagonal;
+}
+
+// Can every velocity contribution be applied inside the step kernel: an
+// explicit matrix (kind 0), or a position commutator with coordinates?
 int plan_aug(E *e, Aug &g) {
     g.inline_v = true;
     for (int64_t a = 0; a < g.ndir; ++a)
         for (int x = 0; x < 3; ++x)
             if (g.dirs[3 * a + x] != 0.) {
                 if (e->vel_kind[x] < 0) return fail(KMSD_EINVAL, "missing Cartesian velocity");
-                if (e->vel_kind[x] != 0) g.inline_v = false;
+                if (e->vel_kind[x] != 0 && !commutator_inline(e, x)) g.inline_v = false;
             }
     g.nvel = 0;
     for (int x = 0; x < 3; ++x) {
@@ -496,12 +575,21 @@ template <class T> void set_inline_v(E *e, StepArgs<T> &a, const Aug &g, double 
     a.nvel = g.nvel;
     for (int v = 0; v < g.nvel; ++v) {
         const int x = g.vel_axis[v];
-        a.Vm[v] = view_of<T>(e->vel[3 * x]);
+        const bool comm = commutator_inline(e, x);
+        a.vform[v] = comm ? 1 : 0;
+        a.xdiag[v] = comm ? e->vel[3 * x]->re64 : nullptr;
+        if (!comm) a.Vm[v] = view_of<T>(e->vel[3 * x]);
         a.vel_axis[v] = x;
         for (int64_t blk = 0; blk < g.ndir; ++blk) {
-            // (-i hbar / half) * dir
-            a.wr[blk][v] = (T)0;
-            a.wi[blk][v] = (T)(-e->hbar / half * g.dirs[3 * blk + x]);
+            if (comm) {
+                // (-i hbar / half) * dir * (i / hbar) on sum_j H_ij (x_j - x_i) psi_j
+                a.wr[blk][v] = (T)(g.dirs[3 * blk + x] / half);
+                a.wi[blk][v] = (T)0;
+            } else {
+                // (-i hbar / half) * dir on V psi
+                a.wr[blk][v] = (T)0;
+                a.wi[blk][v] = (T)(-e->hbar / half * g.dirs[3 * blk + x]);
+            }
         }
     }
 }
@@ -544,7 +632,8 @@ int series_impl(E *e, const double2 *B, double2 *out, int64_t b, const double *c
     if (e->precision == KMSD_MIXED) {
         if (!e->identity) return fail(KMSD_EINVAL, "mixed precision requires an identity metric (orthogonal basis)");
         if (ndir && !g.inline_v)
-            return fail(KMSD_EINVAL, "mixed precision requires explicit velocity matrices (kind 0)");
+            return fail(KMSD_EINVAL, "mixed precision requires explicit velocity matrices (kind 0) or a position "
+                                     "operator given by site coordinates (kind 1, diagonal)");
         if (ndir && g.nb % 2)
             return fail(KMSD_EINVAL, "mixed-precision propagation needs an even number of vectors per block");
         const int U = (int)((b + 1) / 2);
@@ -552,7 +641,7 @@ int series_impl(E *e, const double2 *B, double2 *out, int64_t b, const double *c
             ensure_vec(e->outw, n, U, sizeof(float4)) || e->H->ensure_f32())
             return KMSD_ECUDA;
         for (int v = 0; v < g.nvel; ++v)
-            if (e->vel[3 * g.vel_axis[v]]->ensure_f32()) return KMSD_ECUDA;
+            if (!commutator_inline(e, g.vel_axis[v]) && e->vel[3 * g.vel_axis[v]]->ensure_f32()) return KMSD_ECUDA;
         float4 *ta = e->ta.as<float4>(), *tb = e->tb.as<float4>(), *ow = e->outw.as<float4>();
         if ((rc = to_f32(B, tb, n, b, U, s))) return rc;
         StepArgs<float> a = base_args<float>(e, U, center, half);
@@ -723,6 +812,21 @@ int kmsd_engine_series(kmsd_engine e, const void *b_in, void *out, int64_t b, co
     if (rc) return rc;
     rc = series_impl(e, static_cast<const double2 *>(b_in), static_cast<double2 *>(out), b, coeff, ncoeff, center,
                      half, directions, ndir, s);
+    if (rc) return rc;
+    return finish(e, s);
+}
+
+int kmsd_engine_chain_correlate(kmsd_engine e, const void *b_in, const void *cov, int64_t b, int64_t length,
+                                int64_t kcols, double center, double half, void *tables, void *stream) {
+    if (bad_engine(e) || !b_in || !cov || !tables || b < 1 || kcols < 1)
+        return fail(KMSD_EINVAL, "expected nonempty finite (N,batch) array");
+    if (length < 1) return fail(KMSD_EINVAL, "Chebyshev chain must be nonempty");
+    if (length > 1 && !(half > 0)) return fail(KMSD_EINVAL, "spectral half-width must be positive");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int rc = begin(e, s);
+    if (rc) return rc;
+    rc = correlate_impl(e, static_cast<const double2 *>(b_in), static_cast<const double2 *>(cov), b, length, kcols,
+                        center, half, static_cast<double2 *>(tables), s);
     if (rc) return rc;
     return finish(e, s);
 }

@@ -130,6 +130,22 @@ def canonical(matrix):
     return host
 
 
+def _full_diagonal(X):
+    """A position operator given by site coordinates (only diagonal entries,
+    real) is stored with every diagonal entry explicit, zeros included, so
+    the engine recognises it and applies i [H, X] / hbar from H's rows inside
+    the Chebyshev step; any other matrix is returned unchanged."""
+    A = sp.csr_matrix(X)
+    if A.shape[0] != A.shape[1]:
+        return X
+    coo = A.tocoo()
+    if np.any(coo.row != coo.col) or np.any(np.asarray(coo.data).imag != 0 if np.iscomplexobj(coo.data) else False):
+        return X
+    x = np.asarray(A.diagonal()).real.astype(np.float64)
+    n = A.shape[0]
+    return sp.csr_matrix((x, np.arange(n), np.arange(n + 1)), shape=(n, n))
+
+
 class DeviceCSR:
     """A CSR matrix uploaded to the device; replaces `_native.CSR`."""
 
@@ -167,6 +183,37 @@ class DeviceCSR:
         if h is not None and h.value:
             self.lib.kmsd_csr_destroy(h)
             self.handle = None
+
+
+def vac_nodes(tables, coeffs, G, lib=None):
+    """Per-node spectral tail on the device (kmsd_vac_nodes): `tables` the
+    (b, length, kcols) device tensor of B200Operators.chain_correlate,
+    `coeffs` a list of Bessel coefficient vectors (one per time node, each of
+    at most kcols terms), G the (n_energy, n_moments) reconstruction matrix.
+    Returns the (nodes, b, n_energy) float64 host array of VAC values."""
+    torch = _torch()
+    lib = lib or _abi.require_library()
+    b, length, kcols = tables.shape
+    m = len(coeffs)
+    cf = np.zeros((m, kcols), np.complex128)
+    orders = np.zeros(m, np.int32)
+    for i, c in enumerate(coeffs):
+        if len(c) > kcols:
+            raise ValueError("internal spectral propagation order exceeded segment allocation")
+        cf[i, :len(c)] = c
+        orders[i] = len(c) - 1
+    Gd = torch.from_numpy(np.ascontiguousarray(G, np.float64)).to(tables.device)
+    L, ne = G.shape[1], G.shape[0]
+    if length < L + int(orders.max()):
+        raise ValueError("correlation tables shorter than the moments need")
+    cfd = torch.from_numpy(cf).to(tables.device)
+    od = torch.from_numpy(orders).to(tables.device)
+    nbytes = m * b * (16 * length + 8 * L)
+    work = torch.empty((nbytes + 15) // 16, dtype=torch.complex128, device=tables.device)
+    vac = torch.empty((m, b, ne), dtype=torch.float64, device=tables.device)
+    _check(lib, lib.kmsd_vac_nodes(_ptr(tables.contiguous()), b, length, kcols, L, _ptr(cfd), _ptr(od), m, _ptr(Gd),
+                                   ne, _ptr(work), work.numel() * 16, _ptr(vac), _stream(torch)))
+    return vac.cpu().numpy()
 
 
 def _report_arrays(b):
@@ -427,10 +474,15 @@ class B200Operators:
             kinds[ai] = kind
             for j, m in enumerate(ms):
                 m = m.get() if hasattr(m, "get") and not sp.issparse(m) else m
+                if kind == 1:
+                    m = _full_diagonal(m)
                 d = DeviceCSR(m, self.lib)
                 self._keep.append(d)
                 mats[3 * ai + j] = d.handle
         self._kinds, self._mats, self._config = kinds, mats, config
+        # work done, in applications of the scaled operator to one vector
+        # (orbital.moment.vec / N): moment, propagation and chain steps
+        self.vector_applications = 0
         self._create_engine()
 
     def _create_engine(self):
@@ -535,6 +587,7 @@ class B200Operators:
                                                          len(c), float(center), float(half),
                                                          _dptr(dirs) if nd else None, nd, _stream(torch)),
                    self._failure)
+            self.vector_applications += (len(c) - 1) * x.shape[1]
             if (s0, s1) != (0, nb):
                 out[:, idx] = y
             else:
@@ -557,11 +610,50 @@ class B200Operators:
             y = torch.empty((length, self.n, j1 - j0), dtype=torch.complex128, device=t.device)
             _check(self.lib, self.lib.kmsd_engine_chain(self.handle, _ptr(x), _ptr(y), j1 - j0, int(length),
                                                         float(center), float(half), _stream(torch)), self._failure)
+            self.vector_applications += (length - 1) * (j1 - j0)
             out[:, :, j0:j1] = y
         return _out(out, host)
 
     def chain(self, B, length, center, half):
         return _call(self._chain, B, length, center, half)
+
+    def _chain_correlate(self, B, cov, length, center, half):
+        torch = _torch()
+        t, _ = as_device(B, self.n)
+        b = t.shape[1]
+        cov = cov if isinstance(cov, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(cov, np.complex128))
+        cov = cov.to(t.device, torch.complex128)
+        if length < 1:
+            raise ValueError("Chebyshev chain must be nonempty")
+        if cov.ndim != 3 or cov.shape[0] != self.n or cov.shape[2] != b:
+            raise ValueError("cov must be (N, kcols, batch)")
+        kcols = cov.shape[1]
+        # columns per call: at most 8, fewer when the right chain is long
+        group = 8
+        while group > 1 and kcols > 4 * (256 // group):
+            group //= 2
+        if self.engine_precision == "mixed":
+            group = max(2, group - group % 2)
+        if kcols > 4 * (256 // group):
+            raise ValueError("too many right-chain terms for one correlation call")
+        tables = torch.empty((b, length, kcols), dtype=torch.complex128, device=t.device)
+        for j0 in range(0, b, group):
+            j1 = min(b, j0 + group)
+            x = t[:, j0:j1].contiguous()
+            cv = cov[:, :, j0:j1].contiguous()
+            out = torch.empty((j1 - j0, length, kcols), dtype=torch.complex128, device=t.device)
+            _check(self.lib, self.lib.kmsd_engine_chain_correlate(self.handle, _ptr(x), _ptr(cv), j1 - j0,
+                                                                  int(length), int(kcols), float(center),
+                                                                  float(half), _ptr(out), _stream(torch)),
+                   self._failure)
+            self.vector_applications += (length - 1) * (j1 - j0)
+            tables[j0:j1] = out
+        return tables
+
+    def chain_correlate(self, B, cov, length, center, half):
+        """tables[c, j, k] = <T_j(Ht) B[:, c], cov[:, k, c]> (device tensor of
+        shape (batch, length, kcols)); the chain is never stored whole."""
+        return _call(self._chain_correlate, B, cov, length, center, half)
 
     def _moments(self, B, length, center, half, doubling=None):
         torch = _torch()
@@ -582,6 +674,8 @@ class B200Operators:
                                                                                     C.POINTER(C.c_double)),
                                                           j1 - j0, int(length), float(center), float(half), flags,
                                                           _stream(torch)), self._failure)
+            if length > 1:
+                self.vector_applications += ((length + 1) // 2 if doubling else length - 1) * (j1 - j0)
             mu[:, j0:j1] = m
         return _out(mu, host)
 

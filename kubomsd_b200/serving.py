@@ -87,7 +87,8 @@ class ResidentModel:
     def run(self, req):
         import torch
         c, a = kpm.scaling(self.cfg)
-        B = torch.from_numpy(kpm.random_phases(self.n, req.seed, range(req.vectors))).to("cuda", non_blocking=False)
+        from .devstats import random_phases
+        B = random_phases(self.n, req.seed, range(req.vectors))  # generated on the device
         ops = self.pool.get()
         try:
             if req.kind == "dos":

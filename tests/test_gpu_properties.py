@@ -61,7 +61,8 @@ def test_mixed_moments_error_vs_fp64(lattice):
     _, e32, _ = _eng(m, "mixed")
     ref = e64.moments(B, 1024, 0., 9.2)
     for doubling in (False, True):
-        err = assert_rel(e32.moments(B, 1024, 0., 9.2, doubling=doubling), ref, 1e-4, "mixed moments")
+        # the stated moment tolerance of the mixed form (5e-5, norm-wise)
+        err = assert_rel(e32.moments(B, 1024, 0., 9.2, doubling=doubling), ref, 5e-5, "mixed moments")
         print(f"M=1024 mixed (doubling={doubling}) moments relerr {err:.2e}")
 
 

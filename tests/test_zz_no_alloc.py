@@ -8,8 +8,11 @@ mid-run.  Its workspace is a static 64 MiB device block inside the library.
 Here it is called through the C ABI and compared with `kmsd_engine_moments`
 on the same engine and input, in FP64 and in the mixed form, with both moment
 methods.  It is called twice in a row: the second call starts from the scratch
-contents the first one left behind.  A block too large for the static scratch
-must be rejected, never allocated.
+contents the first one left behind.  Around those two calls the device's free
+memory must not change: the output and the input are allocated, and one
+warm-up call made (it may load the library's device code and with it the
+static block), before the first reading.  A block too large for the static
+scratch must be rejected, never allocated.
 """
 import ctypes as C
 
@@ -22,9 +25,12 @@ pytestmark = pytest.mark.gpu
 HALF = 9.2
 
 
-def _noalloc(lib, eng, B, length, flags, torch):
+def _noalloc(lib, eng, B, length, flags, torch, mu=None):
     from kubomsd_b200 import _abi
-    mu = torch.full((length, B.shape[1]), np.nan, dtype=torch.float64, device="cuda")
+    if mu is None:
+        mu = torch.full((length, B.shape[1]), np.nan, dtype=torch.float64, device="cuda")
+    else:
+        mu.fill_(np.nan)
     rc = lib.kmsd_engine_moments_noalloc(eng.handle, C.c_void_p(B.data_ptr()),
                                          C.cast(C.c_void_p(mu.data_ptr()), C.POINTER(C.c_double)), B.shape[1],
                                          length, 0., HALF, flags, C.c_void_p(torch.cuda.current_stream().cuda_stream))
@@ -46,10 +52,18 @@ def test_noalloc_moments_match_allocating_entry_point(cuda, precision, doubling)
     want = eng.moments(B, 200, 0., HALF, doubling=doubling).cpu().numpy()
     lib = _abi.load()
     flags = _abi.KMSD_MOMENTS_DOUBLING if doubling else _abi.KMSD_MOMENTS_DIRECT
+    mu = torch.empty((200, B.shape[1]), dtype=torch.float64, device="cuda")
+    _noalloc(lib, eng, B, 200, flags, torch, mu)  # warm-up: may load the device code and the static block
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    got = []
     for call in range(2):
-        got = _noalloc(lib, eng, B, 200, flags, torch)
-        assert np.isfinite(got).all()
-        assert_rel(got, want, 1e-10, f"{precision} doubling={doubling} call {call}")
+        got.append(_noalloc(lib, eng, B, 200, flags, torch, mu))
+    free_after = torch.cuda.mem_get_info()[0]
+    assert free_after == free_before, f"device free memory changed by {free_before - free_after} bytes"
+    for call, g in enumerate(got):
+        assert np.isfinite(g).all()
+        assert_rel(g, want, 1e-10, f"{precision} doubling={doubling} call {call}")
 
 
 def test_noalloc_rejects_blocks_beyond_its_scratch(cuda):
