@@ -446,7 +446,7 @@ def config_c2(threads, storage=("fp64", "mixed"), M=1024):
     return out
 
 
-def config_c5(duration=8., rate=20., msd_fraction=.25):
+def config_c5(duration=3., rate=20., msd_fraction=.25):
     """Config 5 (a sampled window): Poisson arrivals at 20 req/s of DOS and
     stepwise-MSD jobs over resident orthogonal lattices (16k-4M sites) and
     nonorthogonal sp3 cells, M in {512, 1024, 2048}, R in {8, 32}, admitted by
@@ -471,6 +471,7 @@ def config_c5(duration=8., rate=20., msd_fraction=.25):
                         + ", ".join(f"{k} ({mm.n:,} orbitals)" for k, mm in models.items())
                         + ", 8 slots, HBM budget 150 GB",
             "latency": latency_summary(res), "requests": len(res), "errors": len(srv.errors),
+            "error_messages": sorted({msg for _, msg in srv.errors})[:5],
             "jobs": {"dos": sum(r.kind == "dos" for r in res), "msd": sum(r.kind == "msd" for r in res)},
             "wall_s": wall, "requests_per_s": len(res) / wall, "offered_rate": rate,
             "slot_occupancy": busy / (8 * wall)}

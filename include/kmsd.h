@@ -329,6 +329,18 @@ int kmsd_engine_moments_noalloc(kmsd_engine e, const void *b_in, double *mu,
                                 int64_t b, int64_t length, double center,
                                 double half, int flags, void *stream);
 
+/* `steps` Lanczos iterations of the pencil (H, S) in the S inner product,
+ * started from the (n, 1) complex128 device vector v0 (S-normalised here):
+ * w = S^-1 H v_j, alpha_j = <v_j, H v_j>, w -= alpha_j v_j + beta_{j-1}
+ * v_{j-1}, beta_j = |w|_S, v_{j+1} = w / beta_j.  alpha and beta are HOST
+ * arrays of `steps` doubles, filled at the end; every step runs on the
+ * device with the scalars kept there, and the call synchronises once.  The
+ * device replacement of the host ARPACK spectral-bound estimate
+ * (src/kubo_msd/metric/bounds.py:26-58); the caller forms the tridiagonal
+ * matrix and truncates at the first negligible beta. */
+int kmsd_engine_lanczos(kmsd_engine e, const void *v0, int64_t steps, double *alpha,
+                        double *beta, void *stream);
+
 /* Reference counters h_calls / v_calls (cpp/native.cpp:718-719). */
 int kmsd_engine_counters(kmsd_engine e, int64_t *h_calls, int64_t *v_calls);
 

@@ -69,6 +69,7 @@ SIGNATURES = {
     "kmsd_engine_series": (C.c_int, [P, P, P, I64, PD, I64, D, D, PD, I64, P]),
     "kmsd_engine_chain": (C.c_int, [P, P, P, I64, I64, D, D, P]),
     "kmsd_engine_chain_correlate": (C.c_int, [P, P, P, I64, I64, I64, D, D, P, P]),
+    "kmsd_engine_lanczos": (C.c_int, [P, P, I64, PD, PD, P]),
     "kmsd_vac_nodes": (C.c_int, [P, I64, I64, I64, I64, P, P, I64, P, I64, P, I64, P, P]),
     "kmsd_random_phases": (C.c_int, [I64, I64, P, P, P]),
     "kmsd_project_moments": (C.c_int, [P, I64, I64, P, I64, P, P]),

@@ -419,13 +419,17 @@ __device__ __forceinline__ void gather_prefetched(const EllRow<T, PF> &r, const 
     }
 }
 
-template <int MU, int MODE, int HSRC>
+#ifndef KMSD_STEP_PAIR_F64
+#define KMSD_STEP_PAIR_F64 1  // the paired form for FP64 vectors too
+#endif
+template <class T, int MU, int MODE, int HSRC>
 constexpr bool step_pairs() {
-    return KMSD_STEP_PAIR && MU == 1 && MODE == MODE_DOUBLING && (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8);
+    return KMSD_STEP_PAIR && (KMSD_STEP_PAIR_F64 || sizeof(T) == 4) && MU == 1 && MODE == MODE_DOUBLING &&
+           (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8);
 }
 
 template <class T, int MU, int MODE, int HSRC, bool INLINE_V>
-__global__ void __launch_bounds__(256, (step_pairs<MU, MODE, HSRC>() ? KMSD_STEP_PAIR_MINB
+__global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_STEP_PAIR_MINB
                                         : MU == 1 && MODE != MODE_SERIES ? KMSD_STEP_MINB : 1))
     cheb_step_kernel(const StepArgs<T> a) {
     using V = typename Unit<T>::vec;
@@ -445,7 +449,7 @@ __global__ void __launch_bounds__(256, (step_pairs<MU, MODE, HSRC>() ? KMSD_STEP
     bool bad = false;
     constexpr int PF = HSRC == HSRC_ELL4 ? 1 : HSRC == HSRC_ELL8 ? 2 : 1;
     const int64_t stride = (int64_t)gridDim.x * mp.gpc;
-    if constexpr (step_pairs<MU, MODE, HSRC>()) {
+    if constexpr (step_pairs<T, MU, MODE, HSRC>()) {
         // Rows `row` and `row + stride` per iteration; the ELL rows of the
         // next pair are loaded one iteration ahead.
         const int u = lane;
@@ -491,10 +495,10 @@ __global__ void __launch_bounds__(256, (step_pairs<MU, MODE, HSRC>() ? KMSD_STEP
         }
     }
     EllRow<T, PF> ahead;
-    if (!step_pairs<MU, MODE, HSRC>() && (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8) &&
+    if (!step_pairs<T, MU, MODE, HSRC>() && (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8) &&
         (int64_t)blockIdx.x * mp.gpc + g < a.n)
         ell_row_load<T, PF>(a.E, (int64_t)blockIdx.x * mp.gpc + g, ahead);
-    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; !step_pairs<MU, MODE, HSRC>() && row < a.n; row += stride) {
+    for (int64_t row = (int64_t)blockIdx.x * mp.gpc + g; !step_pairs<T, MU, MODE, HSRC>() && row < a.n; row += stride) {
         EllRow<T, PF> cur;
         if (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8) {
             cur = ahead;

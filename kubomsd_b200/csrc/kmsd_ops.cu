@@ -18,6 +18,7 @@
 #include "kmsd_impl.h"
 #include "kmsd_kernels.cuh"
 #include "kmsd_tile.cuh"
+#include "kmsd_wave.cuh"
 
 using namespace kmsd;
 
@@ -296,6 +297,170 @@ int to_f64(const float4 *src, double2 *dst, int64_t n, int64_t b, int U, cudaStr
     return KMSD_OK;
 }
 
+// ---------------------------------------------------------------- Lanczos
+// w <- w - alpha v - beta v_prev with alpha = Re dot->x, beta from the device.
+__global__ void lanczos_update_kernel(double2 *w, const double2 *v, const double2 *vp, int64_t n, const double2 *dot,
+                                      const double *beta_prev) {
+    const double al = dot->x, be = beta_prev ? *beta_prev : 0.;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 a = w[i], x = v[i], y = vp[i];
+        w[i] = make_double2(a.x - al * x.x - be * y.x, a.y - al * x.y - be * y.y);
+    }
+}
+// v <- w / beta with beta = sqrt(max(Re dot->x, 0)), recorded in beta_out.
+__global__ void lanczos_scale_kernel(const double2 *w, double2 *v, int64_t n, const double2 *dot, double *beta_out) {
+    const double be = sqrt(fmax(dot->x, 0.));
+    if (beta_out && blockIdx.x == 0 && threadIdx.x == 0) *beta_out = be;
+    const double inv = be > 0. ? 1. / be : 0.;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double2 a = w[i];
+        v[i] = make_double2(a.x * inv, a.y * inv);
+    }
+}
+
+// ---------------------------------------------------------------- two-step launches
+// Per tile of `tr` rows, the range of tiles its rows couple to (from the
+// operator's pattern), on the device as [lo..., hi...]; cached per tile size.
+const int *tile_deps(kmsd_csr_s *A, int tr) {
+    auto it = A->tile_deps.find(tr);
+    if (it != A->tile_deps.end()) return it->second.as<int>();
+    const int64_t ntiles = (A->n + tr - 1) / tr;
+    std::vector<int> h(2 * ntiles);
+    for (int64_t t = 0; t < ntiles; ++t) {
+        int lo = INT32_MAX, hi = -1;
+        for (int64_t r = t * tr; r < std::min<int64_t>(A->n, (t + 1) * tr); ++r) {
+            lo = std::min(lo, A->rowmin[r] / tr);
+            hi = std::max(hi, A->rowmax[r] / tr);
+        }
+        h[t] = lo;
+        h[ntiles + t] = hi;
+    }
+    DevBuf &d = A->tile_deps[tr];
+    if (d.ensure(h.size() * sizeof(int))) return nullptr;
+    if (cudaMemcpy(d.p, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
+    return d.as<int>();
+}
+
+template <class T>
+bool wave_applies(E *e, const StepArgs<T> &a) {
+    static int coop = -1;
+    if (coop < 0) {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        coop = cudaDeviceGetAttribute(&v, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && v ? 1 : 0;
+    }
+    return KMSD_WAVE && coop && a.E.im == nullptr && (a.E.w == 4 || a.E.w == 8) && a.mp.U <= 128 &&
+           mu_for(a.mp) == 1 && !e->H->rowmin.empty();
+}
+
+// Steps k+1 and k+2 of the doubling moments (pairs kmom and kmom + 1) in one
+// cooperative launch of cheb_wave_kernel (kmsd_wave.cuh).
+template <class T, int PF>
+int launch_wave_pf(E *e, const StepArgs<T> &a, typename Unit<T>::vec *X, typename Unit<T>::vec *next,
+                   cudaStream_t s) {
+    const auto kern = cheb_wave_kernel<T, PF>;
+    const int tr = KMSD_WAVE_TILE_ROWS;
+    const int64_t ntiles = (a.n + tr - 1) / tr;
+    const size_t sm = reduce_smem(a.mp, Unit<T>::C);
+    static std::map<size_t, int> per_sm_cache;
+    int per_sm;
+    auto it = per_sm_cache.find(sm);
+    if (it != per_sm_cache.end()) {
+        per_sm = it->second;
+    } else {
+        KMSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)kern, kThreads, sm));
+        per_sm_cache[sm] = per_sm;
+    }
+    if (per_sm < 1) return fail(KMSD_ERUNTIME, "two-step moment kernel cannot be resident");
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)sm_count() * per_sm));
+    const int *deps = tile_deps(e->H, tr);
+    if (!deps) return fail(KMSD_ECUDA, "tile dependency upload failed");
+    if (e->wave_tiles != ntiles || !e->wave_flags.p) {
+        if (e->wave_flags.ensure((size_t)(ntiles + 1) * sizeof(int))) return KMSD_ECUDA;
+        KMSD_CUDA(cudaMemsetAsync(e->wave_flags.p, 0, (size_t)(ntiles + 1) * sizeof(int), s));
+        e->wave_tiles = ntiles;
+        e->wave_epoch = 0;
+    }
+    if (e->red.ensure(grid, a.mp.U * Unit<T>::C, 4)) return KMSD_ECUDA;
+    WaveArgs<T> w;
+    std::memset(&w, 0, sizeof(w));
+    w.n = a.n;
+    w.mp = a.mp;
+    w.E = a.E;
+    w.curr = a.curr;
+    w.prev = a.first ? nullptr : a.prev;
+    w.X = X;
+    w.next = next;
+    w.center = a.center;
+    w.half = a.half;
+    w.inv_half = a.inv_half;
+    w.tr = tr;
+    w.ntiles = ntiles;
+    w.dep_lo = deps;
+    w.dep_hi = deps + ntiles;
+    w.flags = e->wave_flags.as<int>();
+    w.a_done = reinterpret_cast<unsigned *>(e->wave_flags.as<int>() + ntiles);
+    if (++e->wave_epoch <= 0) e->wave_epoch = 1;  // (epochs stay positive; flags start at zero)
+    w.epoch = e->wave_epoch;
+    w.timeout = status_ptr(e) + 3;
+    w.partial = e->red.part();
+    w.ticket = e->red.tick();
+    w.mu = a.mu;
+    w.kmom = a.kmom;
+    w.mlen = a.mlen;
+    w.bcols = a.bcols;
+    void *args[] = {&w};
+    KMSD_CUDA(cudaLaunchCooperativeKernel((const void *)kern, grid, kThreads, args, sm, s));
+    count_launch();
+    return KMSD_OK;
+}
+
+template <class T>
+int launch_wave(E *e, const StepArgs<T> &a, typename Unit<T>::vec *X, typename Unit<T>::vec *next,
+                cudaStream_t s) {
+    return a.E.w == 4 ? launch_wave_pf<T, 1>(e, a, X, next, s) : launch_wave_pf<T, 2>(e, a, X, next, s);
+}
+
+// The doubling moment steps over three work buffers: single steps, or two per
+// launch where the two-step kernel applies.  T_0 = t0 is never written.
+template <class T>
+int doubling_steps(E *e, StepArgs<T> &a, const typename Unit<T>::vec *t0, typename Unit<T>::vec *const (&buf)[3],
+                   int64_t steps, cudaStream_t s) {
+    using V = typename Unit<T>::vec;
+    const bool wave = wave_applies<T>(e, a);
+    const V *curr = t0, *prev = nullptr;
+    auto is_work = [&](const V *p) { return p == buf[0] || p == buf[1] || p == buf[2]; };
+    auto pick = [&](const V *x1, const V *x2, const V *x3) -> V * {
+        for (V *b : buf)
+            if (b != x1 && b != x2 && b != x3) return b;
+        return nullptr;
+    };
+    int rc;
+    for (int64_t k = 0; k < steps;) {
+        a.curr = curr;
+        a.prev = prev;
+        a.first = k == 0;
+        a.kmom = k;
+        if (wave && steps - k >= 2) {
+            V *X = pick(curr, prev, nullptr);
+            V *next = prev && is_work(prev) ? const_cast<V *>(prev) : pick(curr, prev, X);
+            if ((rc = launch_wave<T>(e, a, X, next, s))) return rc;
+            KMSD_CUDA(cudaGetLastError());
+            prev = X;
+            curr = next;
+            k += 2;
+        } else {
+            V *next = prev && is_work(prev) ? const_cast<V *>(prev) : pick(curr, prev, nullptr);
+            a.next = next;
+            if ((rc = launch_step<T, MODE_DOUBLING, true, false>(e, a, s))) return rc;
+            prev = curr;
+            curr = next;
+            k += 1;
+        }
+    }
+    return KMSD_OK;
+}
+
 // ---------------------------------------------------------------- moments
 int moments_impl(E *e, const double2 *B, double *mu, int64_t b, int64_t len, double center, double half, int flags,
                  cudaStream_t s) {
@@ -325,10 +490,17 @@ int moments_impl(E *e, const double2 *B, double *mu, int64_t b, int64_t len, dou
             a.mu = mu;
             a.mlen = len;
             a.bcols = (int)b;
+            const int64_t steps = doubling ? (len + 1) / 2 : len - 1;
+            if (doubling) {
+                if (ensure_vec(e->tc, n, b)) return KMSD_ECUDA;
+                double2 *const wb[3] = {ta, tb, e->tc.as<double2>()};
+                if ((rc = doubling_steps<double>(e, a, B, wb, steps, s))) return rc;
+                e->h_calls += steps;
+                return KMSD_OK;
+            }
             // T0 = B (read only), T1 -> ta, T2 -> tb, then in place over T_{k-2}.
             const double2 *curr = B, *prev = nullptr;
             double2 *bufs[2] = {ta, tb};
-            const int64_t steps = doubling ? (len + 1) / 2 : len - 1;
             for (int64_t k = 1; k <= steps; ++k) {
                 double2 *next = k <= 2 ? bufs[k - 1] : const_cast<double2 *>(prev);
                 a.curr = curr;
@@ -392,6 +564,14 @@ int moments_impl(E *e, const double2 *B, double *mu, int64_t b, int64_t len, dou
     a.bcols = (int)b;
     float4 *curr = tb, *prev = nullptr, *spare = ta;
     const int64_t steps = doubling ? (len + 1) / 2 : len - 1;
+    if (doubling) {
+        if (ensure_vec(e->tc, n, U, sizeof(float4))) return KMSD_ECUDA;
+        // T0 lives in tb; the bra buffer is free under the product identity
+        float4 *const wb[3] = {ta, e->tc.as<float4>(), bra};
+        if ((rc = doubling_steps<float>(e, a, tb, wb, steps, s))) return rc;
+        e->h_calls += steps;
+        return KMSD_OK;
+    }
     for (int64_t k = 1; k <= steps; ++k) {
         float4 *next = k == 1 ? spare : prev;
         a.curr = curr;
@@ -868,6 +1048,73 @@ int kmsd_engine_inner(kmsd_engine e, const void *a, const void *b_in, void *out,
     int rc = spmm64(e->M->S, static_cast<const double2 *>(b_in), e->t1.as<double2>(), b, s);
     if (rc) return rc;
     return coldot64(static_cast<const double2 *>(a), e->t1.as<double2>(), n, b, static_cast<double2 *>(out), s);
+}
+
+int kmsd_engine_lanczos(kmsd_engine e, const void *v0, int64_t steps, double *alpha, double *beta, void *stream) {
+    if (bad_engine(e) || !v0 || !alpha || !beta || steps < 1) return fail(KMSD_EINVAL, "invalid Lanczos arguments");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t n = e->H->n;
+    int rc = begin(e, s);
+    if (rc) return rc;
+    // v, v_prev, H v, w, S w, then the (alpha, beta^2) dots and betas; freed
+    // when the call returns (after its synchronisation on success)
+    DevBuf work;
+    struct Release {
+        DevBuf &b;
+        cudaStream_t s;
+        ~Release() {
+            cudaStreamSynchronize(s);
+            b.release();
+        }
+    } release_work{work, s};
+    if (work.ensure((size_t)5 * n * sizeof(double2) + (size_t)steps * (2 * sizeof(double2) + sizeof(double))))
+        return KMSD_ECUDA;
+    double2 *v = work.as<double2>(), *vp = v + n, *hv = vp + n, *w = hv + n, *sw = w + n;
+    double2 *dots = sw + n;  // [2 steps]: <v, H v>, <w, S w>
+    double *bet = reinterpret_cast<double *>(dots + 2 * steps);
+    const Ctl c{e->rtol, e->atol, e->maxiter};
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sm_count() * 8));
+    // S-normalise the start vector
+    KMSD_CUDA(cudaMemcpyAsync(w, v0, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    KMSD_CUDA(cudaMemsetAsync(vp, 0, n * sizeof(double2), s));
+    const double2 *swp = w;
+    if (!e->identity) {
+        if ((rc = spmm64(e->M->S, w, sw, 1, s))) return rc;
+        swp = sw;
+    }
+    if ((rc = coldot64(w, swp, n, 1, dots + 2 * steps - 1, s))) return rc;  // (scratch slot, overwritten later)
+    lanczos_scale_kernel<<<grid, 256, 0, s>>>(w, v, n, dots + 2 * steps - 1, nullptr);
+    count_launch();
+    for (int64_t j = 0; j < steps; ++j) {
+        // H v; alpha_j = <v, S w> = <v, H v> for w = S^-1 H v
+        if ((rc = spmm64(e->H, v, hv, 1, s))) return rc;
+        if ((rc = coldot64(v, hv, n, 1, dots + 2 * j, s))) return rc;
+        if (e->identity) {
+            KMSD_CUDA(cudaMemcpyAsync(w, hv, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+        } else if ((rc = solve(e, hv, w, 1, c, s))) {
+            return rc;
+        }
+        ++e->h_calls;
+        lanczos_update_kernel<<<grid, 256, 0, s>>>(w, v, vp, n, dots + 2 * j, j ? bet + j - 1 : nullptr);
+        count_launch();
+        swp = w;
+        if (!e->identity) {
+            if ((rc = spmm64(e->M->S, w, sw, 1, s))) return rc;
+            swp = sw;
+        }
+        if ((rc = coldot64(w, swp, n, 1, dots + 2 * j + 1, s))) return rc;
+        // v_prev <- v, v <- w / beta_j
+        KMSD_CUDA(cudaMemcpyAsync(vp, v, n * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+        lanczos_scale_kernel<<<grid, 256, 0, s>>>(w, v, n, dots + 2 * j + 1, bet + j);
+        count_launch();
+    }
+    KMSD_CUDA(cudaGetLastError());
+    std::vector<double2> hd(2 * steps);
+    KMSD_CUDA(cudaMemcpyAsync(hd.data(), dots, 2 * steps * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    KMSD_CUDA(cudaMemcpyAsync(beta, bet, steps * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if ((rc = finish(e, s))) return rc;
+    for (int64_t j = 0; j < steps; ++j) alpha[j] = hd[2 * j].x;
+    return KMSD_OK;
 }
 
 int kmsd_engine_counters(kmsd_engine e, int64_t *h_calls, int64_t *v_calls) {

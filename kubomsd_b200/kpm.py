@@ -233,10 +233,11 @@ def lanczos_spectral_bounds(ops, cfg, steps=160, seed=811):
     """Extremal generalized eigenvalues of (H, S) by Lanczos on the device.
 
     The device replacement of the host ARPACK estimate (bounds.py:26-58) for
-    large operators: `steps` Lanczos iterations in the S inner product with
-    w = S^-1 H v applied by the engine (h_action) and <v, S w> by the
-    engine's inner product, then the extreme Ritz values of the tridiagonal
-    matrix and their residual bounds beta_k |e_k^T y|.  The result goes
+    large operators: `steps` Lanczos iterations in the S inner product
+    (w = S^-1 H v, alpha = <v, H v>, beta = |w|_S) run on the device by
+    kmsd_engine_lanczos with the scalars kept there, then the extreme Ritz
+    values of the tridiagonal matrix and their residual bounds
+    beta_k |e_k^T y|.  The result goes
     through the reference's margin rule: max(1 % of the width, 10 residuals /
     s_lower) on each side, or the enclosure check of user bounds.  Ritz values
     lie inside the spectrum, so the margin is what makes the window enclose
@@ -246,21 +247,14 @@ def lanczos_spectral_bounds(ops, cfg, steps=160, seed=811):
     n = ops.n
     rng = np.random.default_rng(seed)
     v = torch.from_numpy(rng.normal(size=(n, 1)) + 0j).cuda()
-    norm = float(np.sqrt(ops.inner(v, v).cpu().numpy().real[0]))
-    v = v / norm
-    v_prev = torch.zeros_like(v)
+    # every step on the device, one read-back of the scalars at the end
+    a_all, b_all = ops.native.lanczos(v, min(steps, n))
     alphas, betas = [], []
-    beta = 0.
-    for _ in range(min(steps, n)):
-        w = ops.apply_h_action(v)
-        alpha = float(ops.inner(v, w).cpu().numpy().real[0])
-        w = w - alpha * v - beta * v_prev
-        beta = float(np.sqrt(max(ops.inner(w, w).cpu().numpy().real[0], 0.)))
-        alphas.append(alpha)
-        betas.append(beta)
+    for alpha, beta in zip(a_all, b_all):
+        alphas.append(float(alpha))
+        betas.append(float(beta))
         if beta <= 1e-14 * max(abs(alpha), 1.):
             break
-        v_prev, v = v, w / beta
     import scipy.linalg as la
     k = len(alphas)
     T = np.diag(alphas) + np.diag(betas[:k - 1], 1) + np.diag(betas[:k - 1], -1)

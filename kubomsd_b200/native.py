@@ -682,6 +682,18 @@ class B200Operators:
     def moments(self, B, length, center, half, doubling=None):
         return _call(self._moments, B, length, center, half, doubling)
 
+    def lanczos(self, v0, steps):
+        """(alpha, beta) of `steps` Lanczos iterations of (H, S) in the S inner
+        product from v0, run on the device (kmsd_engine_lanczos)."""
+        torch = _torch()
+        v, _ = as_device(v0, self.n, validate=False)
+        v = v[:, :1].contiguous()
+        alpha = np.zeros(int(steps))
+        beta = np.zeros(int(steps))
+        _check(self.lib, self.lib.kmsd_engine_lanczos(self.handle, _ptr(v), int(steps), _dptr(alpha), _dptr(beta),
+                                                      _stream(torch)), self._failure)
+        return alpha, beta
+
     def inner(self, A, B):
         """<A, S B> per column (OperatorBundle.inner, velocity.py:117)."""
         torch = _torch()

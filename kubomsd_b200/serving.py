@@ -13,7 +13,10 @@ same numbers alone and in the mix.
 
 Memory accounting: each model's H, S, velocity and engine set-up is charged
 once when it is loaded.  Each job is charged its recurrence buffers (at most
-six (N, b) blocks) while it runs, and the charge is released when it ends.
+six (N, b) blocks) while it runs, and the charge is released when it ends.  A
+job is admitted only while the charges stay within the HBM budget and the
+device reports the job's bytes free (cudaMemGetInfo), so an estimate that
+falls short of real use delays admission instead of failing a job.
 """
 from __future__ import annotations
 
@@ -115,8 +118,20 @@ class Server:
         self.lock = threading.Condition()
         self.used = 0
         self.busy = 0
+        self.pending_bytes = 0  # admitted, not yet started
         self.results: list[Result] = []
         self.errors: list[tuple[int, str]] = []
+
+    def _device_has(self, need):
+        """The budget is an account of estimates; admission also requires the
+        device to have the job's bytes free right now (cudaMemGetInfo), less
+        what admitted jobs that have not allocated yet may still take (memory
+        cached by the allocator counts as free)."""
+        import torch
+        if self.busy == 0:
+            return True  # nothing running could free more; the allocation itself decides
+        free = torch.cuda.mem_get_info()[0] + torch.cuda.memory_reserved() - torch.cuda.memory_allocated()
+        return free >= need + self.pending_bytes
 
     def _worker(self, work: "queue.Queue", stream):
         import torch
@@ -127,6 +142,8 @@ class Server:
                     return
                 req, admitted = item
                 model = self.models[req.model]
+                with self.lock:
+                    self.pending_bytes -= model.job_bytes(req)
                 try:
                     value = model.run(req)
                     end = time.perf_counter()
@@ -171,10 +188,11 @@ class Server:
                         heapq.heappop(pending)
                         self.errors.append((r.rid, "request exceeds the HBM budget"))
                         continue
-                    if self.used + need > self.budget:
+                    if self.used + need > self.budget or not self._device_has(need):
                         break  # wait for memory (FIFO admission)
                     heapq.heappop(pending)
                     self.used += need
+                    self.pending_bytes += need
                     self.busy += 1
                     # latency counts from the real arrival time
                     r2 = Request(start + r.arrival, r.rid, r.model, r.kind, r.n_moments, r.vectors, r.seed,
