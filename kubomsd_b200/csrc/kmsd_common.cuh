@@ -57,19 +57,6 @@ __device__ __forceinline__ Pk<float> ldg(const float4 *p) {
     r.re[0] = v.x; r.im[0] = v.y; r.re[1] = v.z; r.im[1] = v.w;
     return r;
 }
-// L2-coherent loads (bypassing L1) of data written earlier in the same launch.
-__device__ __forceinline__ Pk<double> ldcg_pk(const double2 *p) {
-    double2 v = __ldcg(p);
-    Pk<double> r;
-    r.re[0] = v.x; r.im[0] = v.y;
-    return r;
-}
-__device__ __forceinline__ Pk<float> ldcg_pk(const float4 *p) {
-    float4 v = __ldcg(p);
-    Pk<float> r;
-    r.re[0] = v.x; r.im[0] = v.y; r.re[1] = v.z; r.im[1] = v.w;
-    return r;
-}
 __device__ __forceinline__ void st(double2 *p, const Pk<double> &a) {
     *p = make_double2(a.re[0], a.im[0]);
 }

@@ -401,17 +401,6 @@ int kmsd_csr_create(int64_t n, const int64_t *indptr, const int64_t *indices, co
             }
             for (; j < w; ++j) ei[r * w + j] = (int)r;  // zero-valued padding on the own row
         }
-        A->rowmin.assign(n, 0);
-        A->rowmax.assign(n, 0);
-        for (int64_t r = 0; r < n; ++r) {
-            int lo = (int)r, hi = (int)r;
-            for (int64_t k = indptr[r]; k < indptr[r + 1]; ++k) {
-                lo = std::min(lo, (int)indices[k]);
-                hi = std::max(hi, (int)indices[k]);
-            }
-            A->rowmin[r] = lo;
-            A->rowmax[r] = hi;
-        }
         rc = up((void **)&A->ell_idx, ei.data(), m * sizeof(int));
         if (!rc) rc = up((void **)&A->ell_re64, er.data(), m * sizeof(double));
         if (!rc && cplx) rc = up((void **)&A->ell_im64, eim.data(), m * sizeof(double));
@@ -487,7 +476,6 @@ void kmsd_csr_destroy(kmsd_csr a) {
     cudaFree(a->bsr_idx);
     cudaFree(a->bsr_re);
     cudaFree(a->bsr_im);
-    for (auto &kv : a->tile_deps) kv.second.release();
     delete a;
 }
 

@@ -82,10 +82,6 @@ struct kmsd_csr_s {
     int64_t bsr_nb = 0;
     int *bsr_ptr = nullptr, *bsr_idx = nullptr;
     double *bsr_re = nullptr, *bsr_im = nullptr;
-    // per row, the smallest and largest column (host), and per tile size the
-    // device ranges of tiles each row tile couples to (two-step moment kernel)
-    std::vector<int> rowmin, rowmax;
-    std::map<int, kmsd::DevBuf> tile_deps;
     int ensure_f32();
     kmsd::CsrView<double> view64() const { return {ptr, idx, re64, complex_values ? im64 : nullptr}; }
     kmsd::CsrView<float> view32() const { return {ptr, idx, re32, complex_values ? im32 : nullptr}; }
@@ -223,10 +219,10 @@ struct kmsd_engine_s {
     bool identity = false;
     kmsd::DevBuf ta, tb, bra, hx, t1, t2, t3, t4, t5, psi, vc, inj[3], outw;
     kmsd::DevBuf ring, corr_partial;  // left-chain ring and partial sums of the correlation tables
-    kmsd::DevBuf tc;                  // third recurrence buffer of the two-step moment kernel
-    kmsd::DevBuf wave_flags;          // per tile phase-A epochs, then the phase-A counter
-    int64_t wave_tiles = 0;
-    int wave_epoch = 0;
+    // per axis, the inline velocity's values aligned with H's ELL columns
+    // (complex, FP64 and FP32 copies); built on first use, -1: cannot align
+    kmsd::DevBuf vell64[3], vell32[3];
+    int vell_state[3] = {0, 0, 0};
     kmsd::DevBuf status;  // int[4]: [0] code, [1] report claim, [2] series nonfinite
     kmsd::DevBuf report;  // FailReportFull
     kmsd::DevBuf dots;    // double2[512]

@@ -351,6 +351,10 @@ template <class T> struct StepArgs {
     CsrView<T> Vm[3];
     int vform[3];
     const double *xdiag[3];
+    // vform[v] = 2: the velocity's values aligned with H's ELL columns
+    // (vel_re/vel_im[row * w + j] pairs with H's ELL index [row * w + j]),
+    // applied from the ELL row the step already holds
+    const T *vel_re[3], *vel_im[3];
     int nvel;              // number of velocity matrices in use
     int vel_axis[3];
     T wr[4][3], wi[4][3];  // injection weights per phi block and velocity matrix
@@ -428,9 +432,13 @@ constexpr bool step_pairs() {
            (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8);
 }
 
+#ifndef KMSD_SERIES_MINB
+#define KMSD_SERIES_MINB 1  // resident CTAs per SM asked for the one-unit series step
+#endif
 template <class T, int MU, int MODE, int HSRC, bool INLINE_V>
 __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_STEP_PAIR_MINB
-                                        : MU == 1 && MODE != MODE_SERIES ? KMSD_STEP_MINB : 1))
+                                        : MU == 1 && MODE != MODE_SERIES ? KMSD_STEP_MINB
+                                        : MU == 1 ? KMSD_SERIES_MINB : 1))
     cheb_step_kernel(const StepArgs<T> a) {
     using V = typename Unit<T>::vec;
     constexpr int C = Unit<T>::C;
@@ -543,8 +551,25 @@ __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_S
                     for (int v = 0; v < a.nvel; ++v) {
                         const T wr = a.wr[blk][v], wi = a.wi[blk][v];
                         if (wr == T(0) && wi == T(0)) continue;
-                        const Pk<T> vp = a.vform[v] ? gather_commutator<T>(a.H, a.xdiag[v], a.curr, row, mp.U, upsi)
-                                                    : gather_unit<T>(a.Vm[v], a.curr, row, mp.U, upsi);
+                        Pk<T> vp;
+                        if ((HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8) && a.vform[v] == 2) {
+                            vp = pk_zero<T>();
+                            const T *vr = a.vel_re[v] + row * (4 * PF), *vi = a.vel_im[v] + row * (4 * PF);
+#pragma unroll
+                            for (int q = 0; q < PF; ++q) {
+                                T r4[4], i4[4];
+                                ld4(vr + 4 * q, r4);
+                                ld4(vi + 4 * q, i4);
+                                const int col[4] = {cur.idx[q].x, cur.idx[q].y, cur.idx[q].z, cur.idx[q].w};
+#pragma unroll
+                                for (int j = 0; j < 4; ++j)
+                                    cmac_cplx(vp, r4[j], i4[j], ldg(a.curr + (size_t)col[j] * mp.U + upsi));
+                            }
+                        } else if (a.vform[v] == 1) {
+                            vp = gather_commutator<T>(a.H, a.xdiag[v], a.curr, row, mp.U, upsi);
+                        } else {
+                            vp = gather_unit<T>(a.Vm[v], a.curr, row, mp.U, upsi);
+                        }
 #pragma unroll
                         for (int c = 0; c < C; ++c) {
                             t.re[c] += wr * vp.re[c] - wi * vp.im[c];

@@ -18,7 +18,6 @@
 #include "kmsd_impl.h"
 #include "kmsd_kernels.cuh"
 #include "kmsd_tile.cuh"
-#include "kmsd_wave.cuh"
 
 using namespace kmsd;
 
@@ -318,149 +317,6 @@ __global__ void lanczos_scale_kernel(const double2 *w, double2 *v, int64_t n, co
     }
 }
 
-// ---------------------------------------------------------------- two-step launches
-// Per tile of `tr` rows, the range of tiles its rows couple to (from the
-// operator's pattern), on the device as [lo..., hi...]; cached per tile size.
-const int *tile_deps(kmsd_csr_s *A, int tr) {
-    auto it = A->tile_deps.find(tr);
-    if (it != A->tile_deps.end()) return it->second.as<int>();
-    const int64_t ntiles = (A->n + tr - 1) / tr;
-    std::vector<int> h(2 * ntiles);
-    for (int64_t t = 0; t < ntiles; ++t) {
-        int lo = INT32_MAX, hi = -1;
-        for (int64_t r = t * tr; r < std::min<int64_t>(A->n, (t + 1) * tr); ++r) {
-            lo = std::min(lo, A->rowmin[r] / tr);
-            hi = std::max(hi, A->rowmax[r] / tr);
-        }
-        h[t] = lo;
-        h[ntiles + t] = hi;
-    }
-    DevBuf &d = A->tile_deps[tr];
-    if (d.ensure(h.size() * sizeof(int))) return nullptr;
-    if (cudaMemcpy(d.p, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
-    return d.as<int>();
-}
-
-template <class T>
-bool wave_applies(E *e, const StepArgs<T> &a) {
-    static int coop = -1;
-    if (coop < 0) {
-        int dev = 0, v = 0;
-        cudaGetDevice(&dev);
-        coop = cudaDeviceGetAttribute(&v, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && v ? 1 : 0;
-    }
-    return KMSD_WAVE && coop && a.E.im == nullptr && (a.E.w == 4 || a.E.w == 8) && a.mp.U <= 128 &&
-           mu_for(a.mp) == 1 && !e->H->rowmin.empty();
-}
-
-// Steps k+1 and k+2 of the doubling moments (pairs kmom and kmom + 1) in one
-// cooperative launch of cheb_wave_kernel (kmsd_wave.cuh).
-template <class T, int PF>
-int launch_wave_pf(E *e, const StepArgs<T> &a, typename Unit<T>::vec *X, typename Unit<T>::vec *next,
-                   cudaStream_t s) {
-    const auto kern = cheb_wave_kernel<T, PF>;
-    const int tr = KMSD_WAVE_TILE_ROWS;
-    const int64_t ntiles = (a.n + tr - 1) / tr;
-    const size_t sm = reduce_smem(a.mp, Unit<T>::C);
-    static std::map<size_t, int> per_sm_cache;
-    int per_sm;
-    auto it = per_sm_cache.find(sm);
-    if (it != per_sm_cache.end()) {
-        per_sm = it->second;
-    } else {
-        KMSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)kern, kThreads, sm));
-        per_sm_cache[sm] = per_sm;
-    }
-    if (per_sm < 1) return fail(KMSD_ERUNTIME, "two-step moment kernel cannot be resident");
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)sm_count() * per_sm));
-    const int *deps = tile_deps(e->H, tr);
-    if (!deps) return fail(KMSD_ECUDA, "tile dependency upload failed");
-    if (e->wave_tiles != ntiles || !e->wave_flags.p) {
-        if (e->wave_flags.ensure((size_t)(ntiles + 1) * sizeof(int))) return KMSD_ECUDA;
-        KMSD_CUDA(cudaMemsetAsync(e->wave_flags.p, 0, (size_t)(ntiles + 1) * sizeof(int), s));
-        e->wave_tiles = ntiles;
-        e->wave_epoch = 0;
-    }
-    if (e->red.ensure(grid, a.mp.U * Unit<T>::C, 4)) return KMSD_ECUDA;
-    WaveArgs<T> w;
-    std::memset(&w, 0, sizeof(w));
-    w.n = a.n;
-    w.mp = a.mp;
-    w.E = a.E;
-    w.curr = a.curr;
-    w.prev = a.first ? nullptr : a.prev;
-    w.X = X;
-    w.next = next;
-    w.center = a.center;
-    w.half = a.half;
-    w.inv_half = a.inv_half;
-    w.tr = tr;
-    w.ntiles = ntiles;
-    w.dep_lo = deps;
-    w.dep_hi = deps + ntiles;
-    w.flags = e->wave_flags.as<int>();
-    w.a_done = reinterpret_cast<unsigned *>(e->wave_flags.as<int>() + ntiles);
-    if (++e->wave_epoch <= 0) e->wave_epoch = 1;  // (epochs stay positive; flags start at zero)
-    w.epoch = e->wave_epoch;
-    w.timeout = status_ptr(e) + 3;
-    w.partial = e->red.part();
-    w.ticket = e->red.tick();
-    w.mu = a.mu;
-    w.kmom = a.kmom;
-    w.mlen = a.mlen;
-    w.bcols = a.bcols;
-    void *args[] = {&w};
-    KMSD_CUDA(cudaLaunchCooperativeKernel((const void *)kern, grid, kThreads, args, sm, s));
-    count_launch();
-    return KMSD_OK;
-}
-
-template <class T>
-int launch_wave(E *e, const StepArgs<T> &a, typename Unit<T>::vec *X, typename Unit<T>::vec *next,
-                cudaStream_t s) {
-    return a.E.w == 4 ? launch_wave_pf<T, 1>(e, a, X, next, s) : launch_wave_pf<T, 2>(e, a, X, next, s);
-}
-
-// The doubling moment steps over three work buffers: single steps, or two per
-// launch where the two-step kernel applies.  T_0 = t0 is never written.
-template <class T>
-int doubling_steps(E *e, StepArgs<T> &a, const typename Unit<T>::vec *t0, typename Unit<T>::vec *const (&buf)[3],
-                   int64_t steps, cudaStream_t s) {
-    using V = typename Unit<T>::vec;
-    const bool wave = wave_applies<T>(e, a);
-    const V *curr = t0, *prev = nullptr;
-    auto is_work = [&](const V *p) { return p == buf[0] || p == buf[1] || p == buf[2]; };
-    auto pick = [&](const V *x1, const V *x2, const V *x3) -> V * {
-        for (V *b : buf)
-            if (b != x1 && b != x2 && b != x3) return b;
-        return nullptr;
-    };
-    int rc;
-    for (int64_t k = 0; k < steps;) {
-        a.curr = curr;
-        a.prev = prev;
-        a.first = k == 0;
-        a.kmom = k;
-        if (wave && steps - k >= 2) {
-            V *X = pick(curr, prev, nullptr);
-            V *next = prev && is_work(prev) ? const_cast<V *>(prev) : pick(curr, prev, X);
-            if ((rc = launch_wave<T>(e, a, X, next, s))) return rc;
-            KMSD_CUDA(cudaGetLastError());
-            prev = X;
-            curr = next;
-            k += 2;
-        } else {
-            V *next = prev && is_work(prev) ? const_cast<V *>(prev) : pick(curr, prev, nullptr);
-            a.next = next;
-            if ((rc = launch_step<T, MODE_DOUBLING, true, false>(e, a, s))) return rc;
-            prev = curr;
-            curr = next;
-            k += 1;
-        }
-    }
-    return KMSD_OK;
-}
-
 // ---------------------------------------------------------------- moments
 int moments_impl(E *e, const double2 *B, double *mu, int64_t b, int64_t len, double center, double half, int flags,
                  cudaStream_t s) {
@@ -490,17 +346,10 @@ int moments_impl(E *e, const double2 *B, double *mu, int64_t b, int64_t len, dou
             a.mu = mu;
             a.mlen = len;
             a.bcols = (int)b;
-            const int64_t steps = doubling ? (len + 1) / 2 : len - 1;
-            if (doubling) {
-                if (ensure_vec(e->tc, n, b)) return KMSD_ECUDA;
-                double2 *const wb[3] = {ta, tb, e->tc.as<double2>()};
-                if ((rc = doubling_steps<double>(e, a, B, wb, steps, s))) return rc;
-                e->h_calls += steps;
-                return KMSD_OK;
-            }
             // T0 = B (read only), T1 -> ta, T2 -> tb, then in place over T_{k-2}.
             const double2 *curr = B, *prev = nullptr;
             double2 *bufs[2] = {ta, tb};
+            const int64_t steps = doubling ? (len + 1) / 2 : len - 1;
             for (int64_t k = 1; k <= steps; ++k) {
                 double2 *next = k <= 2 ? bufs[k - 1] : const_cast<double2 *>(prev);
                 a.curr = curr;
@@ -564,14 +413,6 @@ int moments_impl(E *e, const double2 *B, double *mu, int64_t b, int64_t len, dou
     a.bcols = (int)b;
     float4 *curr = tb, *prev = nullptr, *spare = ta;
     const int64_t steps = doubling ? (len + 1) / 2 : len - 1;
-    if (doubling) {
-        if (ensure_vec(e->tc, n, U, sizeof(float4))) return KMSD_ECUDA;
-        // T0 lives in tb; the bra buffer is free under the product identity
-        float4 *const wb[3] = {ta, e->tc.as<float4>(), bra};
-        if ((rc = doubling_steps<float>(e, a, tb, wb, steps, s))) return rc;
-        e->h_calls += steps;
-        return KMSD_OK;
-    }
     for (int64_t k = 1; k <= steps; ++k) {
         float4 *next = k == 1 ? spare : prev;
         a.curr = curr;
@@ -751,17 +592,89 @@ int plan_aug(E *e, Aug &g) {
     return KMSD_OK;
 }
 
+// The inline velocity of axis x with its values laid out like H's ELL form:
+// entry [r * w + j] is V[r, c] for c = H's ELL column [r * w + j] (zero for
+// padding).  V is the explicit matrix (kind 0) or i [H, X] / hbar for
+// coordinates X (kind 1), formed in FP64 on the host.  Returns false when V
+// has an entry outside H's pattern (the step then gathers V's own rows).
+bool aligned_velocity(E *e, int x) {
+    if (e->vell_state[x]) return e->vell_state[x] > 0;
+    e->vell_state[x] = -1;
+    const kmsd_csr_s *H = e->H, *V = e->vel[3 * x];
+    const int64_t n = H->n, w = H->ell_w;
+    if (w != 4 && w != 8) return false;
+    if (H->complex_values || !V) return false;
+    std::vector<int> eidx(n * w);
+    std::vector<double> eval(n * w);
+    if (cudaMemcpy(eidx.data(), H->ell_idx, eidx.size() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(eval.data(), H->ell_re64, eval.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return false;
+    std::vector<double> re(n * w, 0.), im(n * w, 0.);
+    const bool comm = commutator_inline(e, x);
+    if (comm) {
+        std::vector<double> xs(n);
+        if (cudaMemcpy(xs.data(), V->re64, n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return false;
+        for (int64_t r = 0; r < n; ++r)
+            for (int64_t j = 0; j < w; ++j) {
+                const int c = eidx[r * w + j];
+                im[r * w + j] = eval[r * w + j] * (xs[c] - xs[r]) / e->hbar;  // i H_rc (x_c - x_r) / hbar
+            }
+    } else {
+        std::vector<int> vp(n + 1), vi(std::max<int64_t>(V->nnz, 1));
+        std::vector<double> vr(std::max<int64_t>(V->nnz, 1)), vim(std::max<int64_t>(V->nnz, 1), 0.);
+        if (cudaMemcpy(vp.data(), V->ptr, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(vi.data(), V->idx, V->nnz * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(vr.data(), V->re64, V->nnz * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return false;
+        if (V->complex_values &&
+            cudaMemcpy(vim.data(), V->im64, V->nnz * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return false;
+        for (int64_t r = 0; r < n; ++r)
+            for (int k = vp[r]; k < vp[r + 1]; ++k) {
+                int64_t j = 0;
+                // the first ELL slot of this column that is still unused (a padding
+                // slot points at its own row with a zero value)
+                while (j < w && (eidx[r * w + j] != vi[k] || re[r * w + j] != 0. || im[r * w + j] != 0.)) ++j;
+                if (j == w) return false;
+                re[r * w + j] += vr[k];
+                im[r * w + j] += vim[k];
+            }
+    }
+    std::vector<float> re32(re.begin(), re.end()), im32(im.begin(), im.end());
+    const size_t m = (size_t)n * w;
+    if (e->vell64[x].ensure(2 * m * sizeof(double)) || e->vell32[x].ensure(2 * m * sizeof(float))) return false;
+    double *d64 = e->vell64[x].as<double>();
+    float *d32 = e->vell32[x].as<float>();
+    if (cudaMemcpy(d64, re.data(), m * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d64 + m, im.data(), m * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d32, re32.data(), m * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d32 + m, im32.data(), m * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+        return false;
+    e->vell_state[x] = 1;
+    return true;
+}
+
+template <class T> const T *vell_of(E *e, int x);
+template <> const double *vell_of<double>(E *e, int x) { return e->vell64[x].as<double>(); }
+template <> const float *vell_of<float>(E *e, int x) { return e->vell32[x].as<float>(); }
+
 template <class T> void set_inline_v(E *e, StepArgs<T> &a, const Aug &g, double half) {
     a.nvel = g.nvel;
     for (int v = 0; v < g.nvel; ++v) {
         const int x = g.vel_axis[v];
         const bool comm = commutator_inline(e, x);
-        a.vform[v] = comm ? 1 : 0;
+        const bool aligned = e->identity && aligned_velocity(e, x);
+        a.vform[v] = aligned ? 2 : comm ? 1 : 0;
         a.xdiag[v] = comm ? e->vel[3 * x]->re64 : nullptr;
         if (!comm) a.Vm[v] = view_of<T>(e->vel[3 * x]);
+        if (aligned) {
+            const size_t m = (size_t)e->H->n * e->H->ell_w;
+            a.vel_re[v] = vell_of<T>(e, x);
+            a.vel_im[v] = vell_of<T>(e, x) + m;
+        }
         a.vel_axis[v] = x;
         for (int64_t blk = 0; blk < g.ndir; ++blk) {
-            if (comm) {
+            if (comm && !aligned) {
                 // (-i hbar / half) * dir * (i / hbar) on sum_j H_ij (x_j - x_i) psi_j
                 a.wr[blk][v] = (T)(g.dirs[3 * blk + x] / half);
                 a.wi[blk][v] = (T)0;

@@ -65,3 +65,36 @@ def test_fused_commutator_stepwise_matches_oracle(cuda):
                                     cfg.spectral_bounds, cfg.n_moments, [[1., 0., 0.]], segment_fs=cfg.segment_fs)
     assert_rel(dos, wdos, 1e-10, "dos")
     assert_rel(nums["msd_A2/commutator"], wmsd, 1e-9, "msd")
+
+
+def _honeycomb(Lx=24, Ly=12):
+    from kubomsd_b200 import lattices
+    m = lattices.honeycomb(Lx, Ly, W=1., seed=5)
+    acc = 1.42
+    site = np.arange(m.n)
+    cx, cy = np.divmod(site // 2, Ly)
+    x = acc * 1.5 * (cx + cy) + acc * (site % 2)   # site coordinates along x (no minimum image)
+    return m, {"x": sp.diags(x).tocsr()}
+
+
+@pytest.mark.parametrize("form", ["velocity", "position"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_ell_aligned_velocity_series_matches_oracle(cuda, form, precision):
+    """On a lattice with a 4-wide ELL form the inline velocity (explicit V, or
+    i [H, X] / hbar from coordinates) is applied from H's ELL row with values
+    aligned to its columns; the augmented series matches the oracle."""
+    from kubomsd_b200 import kpm
+    from kubomsd_b200.config import RunConfig
+    from oracle import kpm_oracle as O
+    from tests.gpu_util import engine
+    m, pos = _honeycomb()
+    kw = {"velocity": m.velocity} if form == "velocity" else {"position": pos}
+    B = kpm.random_phases(m.n, 9, range(4))
+    aug = np.concatenate([B, np.zeros_like(B)], axis=1)
+    cfg = RunConfig(energy_eV=[0.], time_fs=[0., 1.], spectral_bounds=(-9.6, 9.6), axes=("x",))
+    coeff, _ = kpm.bessel_coefficients(.5, cfg, weighted_tail=True)
+    c, a = kpm.scaling(cfg)
+    _, eng, _ = engine(m.H, m.S, precision=precision, **kw)
+    got = eng.series(aug, coeff, c, a, [[1., 0., 0.]])
+    want = O.engine_from_model(m.H, m.S, **kw).series(aug, coeff, c, a, [[1., 0., 0.]])
+    assert_rel(got, want, 1e-10 if precision == "fp64" else 5e-5, f"aligned {form} series {precision}")
