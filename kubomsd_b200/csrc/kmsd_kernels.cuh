@@ -426,6 +426,9 @@ __device__ __forceinline__ void gather_prefetched(const EllRow<T, PF> &r, const 
 #ifndef KMSD_STEP_PAIR_F64
 #define KMSD_STEP_PAIR_F64 1  // the paired form for FP64 vectors too
 #endif
+#ifndef KMSD_STEP_PAIR_PREFETCH
+#define KMSD_STEP_PAIR_PREFETCH 0  // rows of the next pair loaded ahead: 0 ELL, 1 + T_{k-2}, 2 + T_{k-1}
+#endif
 template <class T, int MU, int MODE, int HSRC>
 constexpr bool step_pairs() {
     return KMSD_STEP_PAIR && (KMSD_STEP_PAIR_F64 || sizeof(T) == 4) && MU == 1 && MODE == MODE_DOUBLING &&
@@ -460,24 +463,44 @@ __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_S
     if constexpr (step_pairs<T, MU, MODE, HSRC>()) {
         // Rows `row` and `row + stride` per iteration; the ELL rows of the
         // next pair are loaded one iteration ahead.
+        // With KMSD_STEP_PAIR_PREFETCH >= 1 the T_{k-2} rows of the next pair
+        // are loaded one iteration ahead too (>= 2: and its T_{k-1} rows).
+        // The next pair's rows are written only in their own iteration, so the
+        // in-place update is unaffected.
         const int u = lane;
         const int64_t first = (int64_t)blockIdx.x * mp.gpc + g;
+        constexpr int PRE = KMSD_STEP_PAIR_PREFETCH;
+        const bool lane_on = u < mp.U;
         EllRow<T, PF> aheadA, aheadB;
-        if (first < a.n) ell_row_load<T, PF>(a.E, first, aheadA);
-        if (first + stride < a.n) ell_row_load<T, PF>(a.E, first + stride, aheadB);
+        Pk<T> pnA = pk_zero<T>(), pnB = pk_zero<T>(), xnA = pk_zero<T>(), xnB = pk_zero<T>();
+        auto rows_ahead = [&](int64_t rA) {
+            const int64_t rB = rA + stride;
+            if (rA < a.n) ell_row_load<T, PF>(a.E, rA, aheadA);
+            if (rB < a.n) ell_row_load<T, PF>(a.E, rB, aheadB);
+            if (PRE >= 1 && lane_on && !a.first) {
+                if (rA < a.n) pnA = ld(a.prev + (size_t)rA * mp.U + u);
+                if (rB < a.n) pnB = ld(a.prev + (size_t)rB * mp.U + u);
+            }
+            if (PRE >= 2 && lane_on) {
+                if (rA < a.n) xnA = ld(a.curr + (size_t)rA * mp.U + u);
+                if (rB < a.n) xnB = ld(a.curr + (size_t)rB * mp.U + u);
+            }
+        };
+        rows_ahead(first);
         for (int64_t row = first; row < a.n; row += 2 * stride) {
             const int64_t rowB = row + stride;
             const bool hasB = rowB < a.n;
             const EllRow<T, PF> curA = aheadA, curB = aheadB;
-            if (row + 2 * stride < a.n) ell_row_load<T, PF>(a.E, row + 2 * stride, aheadA);
-            if (rowB + 2 * stride < a.n) ell_row_load<T, PF>(a.E, rowB + 2 * stride, aheadB);
-            if (u >= mp.U) continue;
+            const Pk<T> pcA = pnA, pcB = pnB, xcA = xnA, xcB = xnB;
+            rows_ahead(row + 2 * stride);
+            if (!lane_on) continue;
             const size_t oA = (size_t)row * mp.U + u, oB = (size_t)rowB * mp.U + u;
-            const Pk<T> xA = ld(a.curr + oA), pA = a.first ? pk_zero<T>() : ld(a.prev + oA);
+            const Pk<T> xA = PRE >= 2 ? xcA : ld(a.curr + oA);
+            const Pk<T> pA = a.first ? pk_zero<T>() : PRE >= 1 ? pcA : ld(a.prev + oA);
             Pk<T> xB = pk_zero<T>(), pB = pk_zero<T>();
             if (hasB) {
-                xB = ld(a.curr + oB);
-                if (!a.first) pB = ld(a.prev + oB);
+                xB = PRE >= 2 ? xcB : ld(a.curr + oB);
+                if (!a.first) pB = PRE >= 1 ? pcB : ld(a.prev + oB);
             }
             Pk<T> hA[1] = {pk_zero<T>()}, hB[1] = {pk_zero<T>()};
             gather_prefetched<T, 1, PF>(curA, a.curr, mp.U, mp.G, lane, hA);
