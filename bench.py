@@ -449,9 +449,8 @@ def config_c2(threads, storage=("fp64", "mixed"), M=1024):
 def config_c4(threads, ninst=32, R=16, M=64):
     """Config 4 (a sample of the batching form): a ragged batch of `ninst`
     nonorthogonal sp3 instances, cell counts log-uniform in 5..10 (4,000 to
-    32,000 orbitals), on-site disorder W_i ~ U[0.1, 2] eV, kappa(S) about 50
-    (the overlap scale bisected once on a 6^3-cell model and reused),
-    block-Jacobi segmented PCG to rtol 1e-10 with complex64 CG work vectors,
+    32,000 orbitals), on-site disorder W_i ~ U[0.1, 2] eV, kappa(S) = 50 per
+    instance, block-Jacobi segmented PCG to rtol 1e-10 with complex64 CG work vectors,
     R=16, M=64, one batch call; the stated form's 256 instances of up to
     400,000 orbitals are not built (host model generation)."""
     import torch
@@ -462,10 +461,7 @@ def config_c4(threads, ninst=32, R=16, M=64):
     rng = np.random.default_rng(4)
     cells = np.round(np.exp(rng.uniform(np.log(5), np.log(10), ninst))).astype(int)
     W = rng.uniform(.1, 2., ninst)
-    ref_model = lattices.diamond_sp3(cells=6)
-    s_hint = float(ref_model.description.split("s=")[1].split(",")[0])
-    ms = [lattices.diamond_sp3(cells=int(c), W=float(w), seed=100 + i, scale_hint=s_hint)
-          for i, (c, w) in enumerate(zip(cells, W))]
+    ms = [lattices.diamond_sp3(cells=int(c), W=float(w), seed=100 + i) for i, (c, w) in enumerate(zip(cells, W))]
     Ss = [sp.csr_matrix(m.S) for m in ms]
     blocks = [[(a, b, la.cholesky(S[a:b, a:b].toarray(), lower=True)) for a, b in m.atom_slices]
               for m, S in zip(ms, Ss)]
@@ -479,7 +475,7 @@ def config_c4(threads, ninst=32, R=16, M=64):
     s1 = bt.metric.stats()
     out = {"workload": f"config 4 sample: ragged batch of {ninst} nonorthogonal diamond sp3 instances, "
                        f"{min(m.n for m in ms):,}-{max(m.n for m in ms):,} orbitals ({bt.n:,} in total), kappa(S) "
-                       f"about 50, block-Jacobi segmented PCG rtol 1e-10 (complex64 CG vectors), R={R}, M={M}",
+                       f"= 50, block-Jacobi segmented PCG rtol 1e-10 (complex64 CG vectors), R={R}, M={M}",
            "unit": UNIT, "seconds": dt, "value": bt.n * M * R / dt, "gpu_launches": _launches() - l0,
            "segmented_solves": s1.calls - s0.calls,
            "pcg_iterations_per_solve": (s1.max_iterations_sum - s0.max_iterations_sum) / max(s1.calls - s0.calls, 1),

@@ -435,8 +435,12 @@ constexpr bool step_pairs() {
            (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8);
 }
 
+// Resident CTAs per SM asked for the one-unit series step.  On the
+// 4,194,304-site honeycomb with [psi | phi] of 2 x 64 (complex64) or 2 x 32
+// (complex128) columns, 3 (80 registers, no spill) measured 6.04 / 6.41 ms per
+// step against 8.13 / 16.1 ms unbounded and 8.14 / 8.78 ms at 2.
 #ifndef KMSD_SERIES_MINB
-#define KMSD_SERIES_MINB 1  // resident CTAs per SM asked for the one-unit series step
+#define KMSD_SERIES_MINB 3
 #endif
 template <class T, int MU, int MODE, int HSRC, bool INLINE_V>
 __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_STEP_PAIR_MINB
