@@ -57,11 +57,14 @@ def parse():
     p.add_argument("--moments", type=int, default=4096)
     p.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     p.add_argument("--method", choices=["doubling", "direct"], default="doubling")
-    p.add_argument("--workload", choices=["honeycomb", "diamond", "batch", "serving"], default="honeycomb",
+    p.add_argument("--workload", choices=["honeycomb", "diamond", "batch", "serving", "series"],
+                   default="honeycomb",
                    help="honeycomb: the headline KPM-moment workload; diamond: the nonorthogonal sp3 model "
                         "(8000 atoms x 4 orbitals, kappa(S)=50, block-Jacobi PCG to 1e-10, R=32, M=1024); "
                         "batch: a ragged batch of 32 nonorthogonal sp3 instances (4,000-32,000 orbitals), R=16; "
-                        "serving: a Poisson request stream through the continuous-batching service")
+                        "serving: a Poisson request stream through the continuous-batching service; "
+                        "series: the augmented series step of the stepwise MSD alone (honeycomb lx x ly, "
+                        "[psi | phi] = 2 x vectors columns)")
     p.add_argument("--metric-storage", choices=["fp64", "mixed"], default="fp64",
                    help="diamond / batch workloads: storage of the CG work vectors (mixed: complex64, FP64 "
                         "arithmetic, solution, inner products and tests)")
@@ -195,7 +198,14 @@ def run_reference(args):
         return
     from kubomsd_b200 import lattices
     import scipy.sparse as sp
-    m = lattices.honeycomb(args.lx, args.ly, with_velocity=False)
+    n_full = 2 * args.lx * args.ly
+    # The engine's set-up and application times grow in proportion to the
+    # sites (one ELL/CSR pass over vector blocks far larger than the caches),
+    # so each step samples a lattice of the same structure with ly / 4 rows
+    # when the full one would take more than about 3 minutes over the steps
+    # asked for (about 7 us per site for an M=2 call at R=64 on 16 cores).
+    ly = args.ly if n_full * 7e-6 * (args.steps + args.warmup / 6) <= 180 or args.ly < 8 else args.ly // 4
+    m = lattices.honeycomb(args.lx, ly, with_velocity=False)
     threads = len(os.sched_getaffinity(0))
     R, M = args.vectors, args.moments
     B = np.exp(2j * np.pi * np.random.default_rng(9).random((m.n, R)))
@@ -225,17 +235,21 @@ def run_reference(args):
     t_app = max(statistics.median(apps), 1e-9)
     full = t_setup + (M - 1) * t_app
     value = m.n * M * R / full
+    where = (f"the full {m.n:,}-site lattice" if m.n == n_full else
+             f"a {args.lx}x{ly}x2 = {m.n:,}-site honeycomb of the same structure (the {n_full:,}-site step time "
+             f"extrapolated by the site count)")
     cb = {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
           "applications_per_s": m.n * R / t_app, "seconds_per_application": t_app, "setup_seconds": t_setup,
-          "sample": f"Engine::moments on the full {m.n:,}-site lattice, R={R}: warm-up steps are M=1 calls "
+          "sample": f"Engine::moments on {where}, R={R}: warm-up steps are M=1 calls "
                     f"(set-up, min {t_setup:.2f} s), each timed step one M=2 call; the application time is its "
                     f"median minus the set-up ({t_app:.2f} s), and the M={M} call is extrapolated as set-up + "
                     f"{M - 1} applications ({threads} OpenMP threads)"}
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": full * 1e3, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": full * 1e3 * n_full / m.n,
+            "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded lattice and phases)",
             "applications_per_s": m.n * R / t_app,
-            "config": {**config(args, m.n), "reference_sample": cb["sample"]}, "cpu_baseline": cb,
+            "config": {**config(args, n_full), "reference_sample": cb["sample"]}, "cpu_baseline": cb,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -348,7 +362,7 @@ def config_c3_msd(threads, R=64, M=4096, t_end=5.):
     res, dt = _bench_call(lambda: ops.native.series(aug, coeff, c, a, [[1., 0., 0.]]), torch.cuda.synchronize)
     steps = len(coeff) - 1
     cols = 2 * R
-    row_bytes = 5 * cols * 8 + 4 * (4 + 4) + 3 * (4 + 8) + 8  # vectors (complex64) + H ELL row + V row
+    row_bytes = series_row_bytes(cols, 4, 4)  # complex64 vectors, 4-wide ELL rows of H and V
     peak, src = peaks()
     ach = n * row_bytes / (dt / steps) / 1e9
     out["series_step"] = {"seconds_per_1fs_propagation": dt, "steps": steps, "ms_per_step": dt / steps * 1e3,
@@ -599,6 +613,65 @@ def run_diamond(args):
                       "mu0_over_n": float(mu[0].mean().item()) / m.n}))
 
 
+def series_row_bytes(cols, real_bytes, ell_w):
+    """Algorithmic bytes per row of one augmented series step (MODE_SERIES with
+    the velocity applied from H's ELL row): T_k-1 read once (neighbours from
+    cache), T_k-2 read, T_k written, the Bessel accumulator read and written;
+    H's ELL row (column indices and values) and the velocity values aligned
+    with it (real and imaginary planes)."""
+    return 5 * cols * 2 * real_bytes + ell_w * (4 + real_bytes) + 2 * ell_w * real_bytes
+
+
+def run_series(args):
+    """The augmented series step alone: one 1 fs Bessel propagation of
+    [psi | phi] (2R columns) on the honeycomb lx x ly x 2 with its explicit
+    velocity along x, per step; CUDA events around the K timed propagations."""
+    import torch
+    from kubomsd_b200 import _abi, kpm, lattices
+    from kubomsd_b200.config import RunConfig
+    from kubomsd_b200.operators import build_operators
+    lib = _abi.require_library()
+    m = lattices.honeycomb(args.lx, args.ly)
+    n, R = m.n, args.vectors
+    cfg = RunConfig(energy_eV=[0.], time_fs=[0., 1.], spectral_bounds=BOUNDS, axes=("x",), include_vac=False,
+                    precision=args.precision)
+    ops = build_operators(m, cfg)
+    B = devstats_phases(n, 20261019, range(R))
+    aug = torch.cat([B, torch.zeros_like(B)], dim=1).contiguous()
+    coeff, _ = kpm.bessel_coefficients(1., cfg, weighted_tail=True)
+    c, a = kpm.scaling(cfg)
+    for _ in range(max(args.warmup, 1)):
+        res = ops.native.series(aug, coeff, c, a, [[1., 0., 0.]])
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    clocks = Clocks(torch.cuda.current_device())
+    l0 = lib.kmsd_kernel_launches()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(args.steps):
+        res = ops.native.series(aug, coeff, c, a, [[1., 0., 0.]])
+    e.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = s.elapsed_time(e) / args.steps
+    bessel = len(coeff) - 1
+    nnz = int(np.diff(m.H.tocsr().indptr).max())
+    rb = series_row_bytes(2 * R, 4 if args.precision == "mixed" else 8, 4 if nnz <= 4 else 8 if nnz <= 8 else nnz)
+    peak, src = peaks()
+    ach = n * rb / (ms / bessel / 1e3) / 1e9
+    print(json.dumps({"metric": "augmented series step (1 fs Bessel propagation of [psi | phi])",
+                      "value": n * 2 * R * bessel / (ms / 1e3), "unit": "orbital·vec·step/s", "n_gpus": 1,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                      "dtype": "c64" if args.precision == "mixed" else "c128", "data": "synthetic (seeded lattice)",
+                      "config": {"workload": f"series step, honeycomb {args.lx}x{args.ly}x2 = {n:,} sites, "
+                                             f"[psi | phi] = 2 x {R} columns, explicit velocity along x",
+                                 "precision": args.precision, "bessel_steps": bessel},
+                      "ms_per_bessel_step": ms / bessel, "gpu_launches": int(lib.kmsd_kernel_launches() - l0),
+                      "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                                   "peak_source": peak_src_note(src), "algorithmic_bytes_per_row": rb},
+                      "clocks": clk, "checksum": float(res.abs().square().sum().item())}))
+
+
 def run_batch(args):
     """Ragged batch of nonorthogonal instances (a sample of the 256-instance,
     4k-400k-orbital batching config): 32 diamond sp3 instances with
@@ -731,6 +804,9 @@ def main():
         return
     if args.workload == "batch":
         run_batch(args)
+        return
+    if args.workload == "series":
+        run_series(args)
         return
     import torch
     import torch.distributed as dist
