@@ -192,6 +192,20 @@ def cpu_baseline(H, n, threads, R=64, M=M_FULL, setup=None):
                       f"{threads} OpenMP threads; the M={M} call extrapolated as set-up + {M - 1} applications"}
 
 
+def reference_sample_ly(lx, ly, steps, warmup, budget_s=180., s_per_site=7e-6):
+    """Rows of the honeycomb the reference arm samples.  The engine's set-up
+    and application times grow in proportion to the sites (every pass streams
+    vector blocks far larger than the host caches), so when the full lattice
+    would take more than `budget_s` over the steps asked for (about 7 us per
+    site for an M=2 call at R=64 on 16 cores; an M=1 warm-up call is about a
+    sixth of that) each step samples a lattice of the same structure with
+    ly / 4 rows."""
+    n_full = 2 * lx * ly
+    if n_full * s_per_site * (steps + warmup / 6) <= budget_s or ly < 8:
+        return ly
+    return ly // 4
+
+
 def run_reference(args):
     world, rank, _ = dist_setup(args)
     if rank != 0:
@@ -199,12 +213,7 @@ def run_reference(args):
     from kubomsd_b200 import lattices
     import scipy.sparse as sp
     n_full = 2 * args.lx * args.ly
-    # The engine's set-up and application times grow in proportion to the
-    # sites (one ELL/CSR pass over vector blocks far larger than the caches),
-    # so each step samples a lattice of the same structure with ly / 4 rows
-    # when the full one would take more than about 3 minutes over the steps
-    # asked for (about 7 us per site for an M=2 call at R=64 on 16 cores).
-    ly = args.ly if n_full * 7e-6 * (args.steps + args.warmup / 6) <= 180 or args.ly < 8 else args.ly // 4
+    ly = reference_sample_ly(args.lx, args.ly, args.steps, args.warmup)
     m = lattices.honeycomb(args.lx, ly, with_velocity=False)
     threads = len(os.sched_getaffinity(0))
     R, M = args.vectors, args.moments

@@ -206,6 +206,24 @@ def pcg_known():
     return out
 
 
+def statistics_case():
+    """The reference's paired block bootstrap (observables/statistics.py:5-22)
+    on seeded block sums: 9 blocks of unequal counts over (axis, time,
+    energy), a denominator of shape (blocks, 1) broadcast over the energies,
+    and one energy whose denominator vanishes in some resamples."""
+    from kubo_msd.observables.statistics import estimate_ratio
+    rng = np.random.default_rng(3)
+    out = {"A": rng.random((9, 2, 4, 7)), "D": rng.random((9, 7)) + .5, "counts": rng.integers(1, 5, 9)}
+    out["value"], out["stderr"], _ = estimate_ratio(out["A"], out["D"], out["counts"])
+    out["A2"], out["D2"], out["counts2"] = rng.random((5, 6)), rng.random((5, 1)) + .2, np.array([3, 1, 4, 1, 5])
+    out["value2"], out["stderr2"], _ = estimate_ratio(out["A2"], out["D2"], out["counts2"])
+    D3 = rng.random((4, 3)) + .1
+    D3[1:, 2] = 0.
+    out["A3"], out["D3"], out["counts3"] = rng.random((4, 3)), D3, np.array([2, 2, 2, 2])
+    out["value3"], out["stderr3"], _ = estimate_ratio(out["A3"], out["D3"], out["counts3"])
+    return out
+
+
 def host_formulas():
     out = {}
     cfg = base_config(spectral_bounds=(-11.2, 11.2))
@@ -362,6 +380,7 @@ CASES = {
        for kind in ("velocity", "position", "composite") for pre in ("diagonal", "block-jacobi")},
     "pcg_known": pcg_known,
     "host_formulas": host_formulas,
+    "statistics": statistics_case,
     "square16_pipeline": square_pipeline,
     "square16_pipeline_vac": lambda: square_pipeline("stepwise", include_vac=True),
     "square16_pipeline_spectral": lambda: square_pipeline("spectral", include_vac=False),

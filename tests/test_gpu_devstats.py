@@ -52,6 +52,21 @@ def test_device_bootstrap_broadcast_counts(cuda):
     np.testing.assert_allclose(se.cpu().numpy(), se_host, rtol=1e-11)
 
 
+@pytest.mark.parametrize("tag", ["", "2", "3"])
+def test_device_bootstrap_matches_reference_golden(cuda, tag):
+    """The device bootstrap against the reference's estimate_ratio run on the
+    same blocks (tests/golden/statistics.npz): unequal counts, a broadcast
+    (blocks, 1) denominator, and resamples with a vanishing denominator."""
+    from kubomsd_b200 import devstats
+    from tests.helpers import golden
+    torch = cuda
+    d = golden("statistics")
+    v, se, _ = devstats.estimate_ratio(torch.from_numpy(d["A" + tag]).cuda(), torch.from_numpy(d["D" + tag]).cuda(),
+                                       d["counts" + tag])
+    np.testing.assert_allclose(v.cpu().numpy(), d["value" + tag], rtol=1e-13)
+    np.testing.assert_allclose(se.cpu().numpy(), d["stderr" + tag], rtol=1e-11, equal_nan=True)
+
+
 def test_device_projection_matches_host(cuda):
     from kubomsd_b200 import devstats, kpm
     torch = cuda
