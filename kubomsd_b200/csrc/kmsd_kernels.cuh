@@ -26,9 +26,14 @@ __device__ __forceinline__ void cmac_cplx(Pk<T> &acc, T vr, T vi, const Pk<T> &x
         acc.im[c] = fma(vr, x.im[c], fma(vi, x.re[c], acc.im[c]));
     }
 }
-// a / s for real s: IEEE division in FP64 (the reference divides by the
-// spectral half-width), multiplication by the reciprocal in FP32.
-__device__ __forceinline__ double rdiv(double a, double s, double) { return a / s; }
+// The spectral rescaling (h - c x) / half.  FP64 divides as the reference's
+// Engine::scaled does (native.cpp:534-538) unless KMSD_F64_RECIP is set, which
+// multiplies by the rounded reciprocal (at most one rounding apart per step);
+// FP32 multiplies by the reciprocal.
+#ifndef KMSD_F64_RECIP
+#define KMSD_F64_RECIP 0
+#endif
+__device__ __forceinline__ double rdiv(double a, double s, double inv) { return KMSD_F64_RECIP ? a * inv : a / s; }
 __device__ __forceinline__ float rdiv(float a, float, float inv) { return a * inv; }
 
 // acc[m] += sum_k A[row,k] X[k, unit u_m]   for the MU units of this lane.
@@ -356,6 +361,7 @@ template <class T> struct StepArgs {
     // applied from the ELL row the step already holds
     const T *vel_re[3], *vel_im[3];
     int nvel;              // number of velocity matrices in use
+    int share_v;           // every velocity in use has vform 2: psi lanes share V psi (see gather_share_v)
     int vel_axis[3];
     T wr[4][3], wi[4][3];  // injection weights per phi block and velocity matrix
     // precomputed injection (general path): inj[a] of shape (n, UR units), FP64 complex
@@ -442,6 +448,74 @@ constexpr bool step_pairs() {
 #ifndef KMSD_SERIES_MINB
 #define KMSD_SERIES_MINB 3
 #endif
+// The series step loads a row's Bessel accumulator with its other row-local
+// operands, before the gathers, instead of after the row's arithmetic.
+#ifndef KMSD_SERIES_EARLY_OUT
+#define KMSD_SERIES_EARLY_OUT 1
+#endif
+// Series step over a 4- or 8-wide ELL operator with every velocity aligned to
+// H's ELL columns: the psi lanes form the velocity products V_v psi from the
+// neighbour values they gather for H anyway and leave them in shared memory
+// (two parity slices of nvel x blockDim.x units) for the phi lanes of their
+// row group, which then gather only their own H row.
+// On the 4,194,304-site honeycomb with [psi | phi] of 2 x 64 complex64 columns
+// the series step took 5.08 ms with the shared products against 5.44 ms
+// without (6.04 ms before the early accumulator load); with 2 x 32 complex128
+// columns it took 6.46 against 6.41 ms (a 68-byte spill under the register
+// bound), so the FP64 step keeps its own gathers.
+#ifndef KMSD_SERIES_SHARE_V
+#define KMSD_SERIES_SHARE_V 1
+#endif
+#ifndef KMSD_SERIES_SHARE_V_F64
+#define KMSD_SERIES_SHARE_V_F64 0
+#endif
+template <class T> constexpr bool series_shares_v() {
+    return KMSD_SERIES_SHARE_V && (sizeof(T) == 4 || KMSD_SERIES_SHARE_V_F64);
+}
+template <class T, int PF>
+__device__ __forceinline__ void gather_share_v(const StepArgs<T> &a, const EllRow<T, PF> &r, int64_t row, int u,
+                                               Pk<T> &acc, typename Unit<T>::vec *slot) {
+    const int U = a.mp.U;
+    if (u >= U) return;
+    Pk<T> xs[PF][4];
+#pragma unroll
+    for (int q = 0; q < PF; ++q) {
+        const int col[4] = {r.idx[q].x, r.idx[q].y, r.idx[q].z, r.idx[q].w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) xs[q][j] = ldg(a.curr + (size_t)col[j] * U + u);
+    }
+#pragma unroll
+    for (int q = 0; q < PF; ++q)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) cmac_real(acc, r.val[q][j], xs[q][j]);
+    if (u >= a.UR) return;
+#pragma unroll 1
+    for (int v = 0; v < a.nvel; ++v) {
+        Pk<T> vp = pk_zero<T>();
+        const T *vr = a.vel_re[v] + row * (4 * PF), *vi = a.vel_im[v] + row * (4 * PF);
+#pragma unroll
+        for (int q = 0; q < PF; ++q) {
+            T r4[4], i4[4];
+            ld4(vr + 4 * q, r4);
+            ld4(vi + 4 * q, i4);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) cmac_cplx(vp, r4[j], i4[j], xs[q][j]);
+        }
+        st(slot + (size_t)v * blockDim.x, vp);
+    }
+}
+// Barrier over one row group: a named barrier for groups of several warps,
+// the group's lanes of the warp otherwise (a group shares its trip count).
+__device__ __forceinline__ void group_sync(const RowMap &mp, int g) {
+    if (mp.G > 32) {
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(mp.G) : "memory");
+    } else {
+        const unsigned lanes =
+            mp.G == 32 ? 0xffffffffu : ((1u << mp.G) - 1u) << ((threadIdx.x & 31) / mp.G * mp.G);
+        __syncwarp(lanes);
+    }
+}
+
 template <class T, int MU, int MODE, int HSRC, bool INLINE_V>
 __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_STEP_PAIR_MINB
                                         : MU == 1 && MODE != MODE_SERIES ? KMSD_STEP_MINB
@@ -529,6 +603,11 @@ __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_S
             }
         }
     }
+    constexpr bool SHARE = series_shares_v<T>() && MODE == MODE_SERIES && INLINE_V && MU == 1 &&
+                           (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8);
+    const bool share = SHARE && a.share_v;
+    V *const vshare = reinterpret_cast<V *>(smem);
+    int parity = 0;
     EllRow<T, PF> ahead;
     if (!step_pairs<T, MU, MODE, HSRC>() && (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8) &&
         (int64_t)blockIdx.x * mp.gpc + g < a.n)
@@ -539,8 +618,9 @@ __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_S
             cur = ahead;
             if (row + stride < a.n) ell_row_load<T, PF>(a.E, row + stride, ahead);
         }
-        // Row-local operands first, so their latency overlaps the gathers.
-        Pk<T> xo[MU], po[MU];
+        // Row-local operands first, so their latency overlaps the gathers
+        // (the series accumulator too, when this row adds to it).
+        Pk<T> xo[MU], po[MU], oo[MODE == MODE_SERIES ? MU : 1];
 #pragma unroll
         for (int m = 0; m < MU; ++m) {
             const int u = lane + m * mp.G;
@@ -548,16 +628,28 @@ __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_S
                 const size_t o = (size_t)row * mp.U + u;
                 xo[m] = ld(a.curr + o);
                 po[m] = a.first ? pk_zero<T>() : ld(a.prev + o);
+                if (MODE == MODE_SERIES && KMSD_SERIES_EARLY_OUT) oo[m] = a.first ? pk_zero<T>() : ld(a.out + o);
             }
         }
         Pk<T> h[MU];
         if (HSRC != HSRC_SOLVED) {
 #pragma unroll
             for (int m = 0; m < MU; ++m) h[m] = pk_zero<T>();
-            if (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8) gather_prefetched<T, MU, PF>(cur, a.curr, mp.U, mp.G, lane, h);
-            else if (HSRC == HSRC_ELL) gather_row_ell<T, MU>(a.E, a.curr, row, mp.U, mp.G, lane, h);
-            else gather_row<T, MU>(a.H, a.curr, row, mp.U, mp.G, lane, h);
+            if constexpr (SHARE) {
+                if (share)
+                    gather_share_v<T, PF>(a, cur, row, lane, h[0],
+                                          vshare + (size_t)parity * a.nvel * blockDim.x + threadIdx.x);
+                else
+                    gather_prefetched<T, MU, PF>(cur, a.curr, mp.U, mp.G, lane, h);
+            } else if (HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8) {
+                gather_prefetched<T, MU, PF>(cur, a.curr, mp.U, mp.G, lane, h);
+            } else if (HSRC == HSRC_ELL) {
+                gather_row_ell<T, MU>(a.E, a.curr, row, mp.U, mp.G, lane, h);
+            } else {
+                gather_row<T, MU>(a.H, a.curr, row, mp.U, mp.G, lane, h);
+            }
         }
+        if (SHARE && share) group_sync(mp, g);
 #pragma unroll
         for (int m = 0; m < MU; ++m) {
             const int u = lane + m * mp.G;
@@ -579,7 +671,9 @@ __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_S
                         const T wr = a.wr[blk][v], wi = a.wi[blk][v];
                         if (wr == T(0) && wi == T(0)) continue;
                         Pk<T> vp;
-                        if ((HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8) && a.vform[v] == 2) {
+                        if (SHARE && share) {
+                            vp = ld(vshare + ((size_t)parity * a.nvel + v) * blockDim.x + g * mp.G + upsi);
+                        } else if ((HSRC == HSRC_ELL4 || HSRC == HSRC_ELL8) && a.vform[v] == 2) {
                             vp = pk_zero<T>();
                             const T *vr = a.vel_re[v] + row * (4 * PF), *vi = a.vel_im[v] + row * (4 * PF);
 #pragma unroll
@@ -651,7 +745,7 @@ __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_S
                         ov.im[c] = a.c0r * x.im[c] + a.c0i * x.re[c] + a.ckr * nx.im[c] + a.cki * nx.re[c];
                     }
                 } else {
-                    ov = ld(a.out + o);
+                    ov = KMSD_SERIES_EARLY_OUT ? oo[MODE == MODE_SERIES ? m : 0] : ld(a.out + o);
 #pragma unroll
                     for (int c = 0; c < C; ++c) {
                         ov.re[c] += a.ckr * nx.re[c] - a.cki * nx.im[c];
@@ -663,6 +757,9 @@ __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_S
                 st(a.out + o, ov);
             }
         }
+        // the next row writes the other slice; this row's readers are done
+        // with it once they reach the next row's barrier
+        if (SHARE) parity ^= 1;
     }
     if (MODE == MODE_SERIES) {
         if (bad) atomicOr(a.status, 1);

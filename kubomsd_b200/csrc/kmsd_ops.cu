@@ -153,7 +153,9 @@ int v_cov(E *e, const double *dir, const double2 *B, double2 *out, int64_t b, co
 template <class T, int MU, int MODE, int HSRC, bool IV>
 int launch_step_mu(E *e, StepArgs<T> &a, cudaStream_t s) {
     const auto kern = cheb_step_kernel<T, MU, MODE, HSRC, IV>;
-    const size_t sm = reduce_smem(a.mp, Unit<T>::C);
+    size_t sm = reduce_smem(a.mp, Unit<T>::C);
+    if (MODE == MODE_SERIES && a.share_v)  // two parity slices of the shared velocity products
+        sm = std::max(sm, (size_t)2 * a.nvel * kThreads * sizeof(typename Unit<T>::vec));
     const int grid = wave_grid((const void *)kern, sm, a.n, a.mp);
     if (MODE == MODE_DIRECT || MODE == MODE_DOUBLING) {
         if (e->red.ensure(grid, a.mp.U * Unit<T>::C, 2)) return KMSD_ECUDA;
@@ -685,6 +687,8 @@ template <class T> void set_inline_v(E *e, StepArgs<T> &a, const Aug &g, double 
             }
         }
     }
+    a.share_v = series_shares_v<T>() && a.nvel > 0;
+    for (int v = 0; v < a.nvel; ++v) a.share_v &= a.vform[v] == 2;
 }
 
 // Injection buffers inj[a] = S^-1 v_cov(dir_a, psi) for the general path.

@@ -44,6 +44,29 @@ namespace kmsd {
 #define KMSD_TILE_WAIT_NS 2000000000ull  // 2 s
 #endif
 
+#ifndef KMSD_TILE_VEC
+#define KMSD_TILE_VEC 1  // vector loads of a row's ELL entries from the stage, 32-bit in-tile offsets
+#endif
+
+// W ELL values of one row from the stage (16-byte aligned: the values region
+// starts on a 16-byte boundary and a row holds 4 or 8 entries).
+template <class T, int W>
+__device__ __forceinline__ void tile_vals(const T *p, T (&v)[W]) {
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int k = 0; k < W / 4; ++k) {
+            const float4 q = reinterpret_cast<const float4 *>(p)[k];
+            v[4 * k] = q.x; v[4 * k + 1] = q.y; v[4 * k + 2] = q.z; v[4 * k + 3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < W / 2; ++k) {
+            const double2 q = reinterpret_cast<const double2 *>(p)[k];
+            v[2 * k] = q.x; v[2 * k + 1] = q.y;
+        }
+    }
+}
+
 constexpr int kTileConsumers = 256;                    // eight consumer warps
 constexpr int kTileThreads = kTileConsumers + 32;      // plus one producer warp
 constexpr int kTileMaxRows = 256;
@@ -223,19 +246,40 @@ __global__ void __launch_bounds__(kTileThreads, KMSD_TILE_MINB)
                 // KMSD_TILE_RB rows of this row group at a time: all their
                 // neighbour loads are issued before any of them is computed
                 constexpr int RB = KMSD_TILE_RB;
+                const int t0i = (int)t0;  // rows and column indices are int32
                 for (int r = g; r < rows; r += RB * mp.gpc) {
                     Pk<T> xg[RB][W];
 #pragma unroll
                     for (int q = 0; q < RB; ++q) {
                         const int rr = r + q * mp.gpc;
                         if (rr >= rows) break;
+                        if (KMSD_TILE_VEC) {
+                            // the row's indices as int4 (16-byte aligned in the stage);
+                            // in-tile offsets in 32 bits
+                            int cols[W];
 #pragma unroll
-                        for (int j = 0; j < W; ++j) {
-                            const int col = is[rr * W + j];
-                            const int64_t lc = (int64_t)col - t0;
-                            const V *src = (uint64_t)lc < (uint64_t)rows ? xs + lc * U + u
-                                                                          : a.curr + (int64_t)col * U + u;
-                            xg[q][j] = ld(src);
+                            for (int j4 = 0; j4 < W / 4; ++j4) {
+                                const int4 c4 = reinterpret_cast<const int4 *>(is + rr * W)[j4];
+                                cols[4 * j4] = c4.x;
+                                cols[4 * j4 + 1] = c4.y;
+                                cols[4 * j4 + 2] = c4.z;
+                                cols[4 * j4 + 3] = c4.w;
+                            }
+#pragma unroll
+                            for (int j = 0; j < W; ++j) {
+                                const unsigned lc = (unsigned)(cols[j] - t0i);
+                                xg[q][j] = lc < (unsigned)rows ? ld(xs + (int)lc * U + u)
+                                                               : ldg(a.curr + (int64_t)cols[j] * U + u);
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < W; ++j) {
+                                const int col = is[rr * W + j];
+                                const int64_t lc = (int64_t)col - t0;
+                                const V *src = (uint64_t)lc < (uint64_t)rows ? xs + lc * U + u
+                                                                              : a.curr + (int64_t)col * U + u;
+                                xg[q][j] = ld(src);
+                            }
                         }
                     }
 #pragma unroll
@@ -243,8 +287,15 @@ __global__ void __launch_bounds__(kTileThreads, KMSD_TILE_MINB)
                         const int rr = r + q * mp.gpc;
                         if (rr >= rows) break;
                         Pk<T> h = pk_zero<T>();
+                        if (KMSD_TILE_VEC) {
+                            T vals[W];
+                            tile_vals<T, W>(vs + rr * W, vals);
 #pragma unroll
-                        for (int j = 0; j < W; ++j) cmac_real(h, vs[rr * W + j], xg[q][j]);
+                            for (int j = 0; j < W; ++j) cmac_real(h, vals[j], xg[q][j]);
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < W; ++j) cmac_real(h, vs[rr * W + j], xg[q][j]);
+                        }
                         const Pk<T> x = ld(xs + rr * U + u);
                         const Pk<T> pv = has_prev ? ld(ps + rr * U + u) : pk_zero<T>();
                         Pk<T> nx;

@@ -98,3 +98,35 @@ def test_ell_aligned_velocity_series_matches_oracle(cuda, form, precision):
     got = eng.series(aug, coeff, c, a, [[1., 0., 0.]])
     want = O.engine_from_model(m.H, m.S, **kw).series(aug, coeff, c, a, [[1., 0., 0.]])
     assert_rel(got, want, 1e-10 if precision == "fp64" else 5e-5, f"aligned {form} series {precision}")
+
+
+@pytest.mark.parametrize("R", [16, 32, 64])
+@pytest.mark.parametrize("form", ["velocity", "position"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_ell_aligned_series_wide_blocks(cuda, R, form, precision):
+    """[psi | phi] blocks of R columns each make row groups of 16 to 128 lanes
+    (one to four warps); the psi lanes' velocity products reach the phi lanes
+    through shared memory under a warp or named barrier.  The position form
+    takes two directions (x and a diagonal), so two velocity matrices feed
+    each of its two phi blocks."""
+    from kubomsd_b200 import kpm
+    from kubomsd_b200.config import RunConfig
+    from oracle import kpm_oracle as O
+    from tests.gpu_util import engine
+    m, pos = _honeycomb()
+    site = np.arange(m.n)
+    cx, cy = np.divmod(site // 2, 12)
+    pos["y"] = sp.diags(1.42 * .866 * (cy - cx) + .71 * (site % 2)).tocsr()
+    if form == "velocity":
+        kw, dirs, axes = {"velocity": m.velocity}, [[1., 0., 0.]], ("x",)
+    else:
+        kw, dirs, axes = {"position": pos}, [[1., 0., 0.], [.6, .8, 0.]], ("x", "y")
+    B = kpm.random_phases(m.n, 11, range(R))
+    aug = np.concatenate([B] + [np.zeros_like(B)] * len(dirs), axis=1)
+    cfg = RunConfig(energy_eV=[0.], time_fs=[0., 1.], spectral_bounds=(-9.6, 9.6), axes=axes)
+    coeff, _ = kpm.bessel_coefficients(.5, cfg, weighted_tail=True)
+    c, a = kpm.scaling(cfg)
+    _, eng, _ = engine(m.H, m.S, precision=precision, **kw)
+    got = eng.series(aug, coeff, c, a, dirs)
+    want = O.engine_from_model(m.H, m.S, **kw).series(aug, coeff, c, a, dirs)
+    assert_rel(got, want, 1e-10 if precision == "fp64" else 5e-5, f"aligned {form} series R={R} {precision}")
