@@ -435,6 +435,9 @@ __device__ __forceinline__ void gather_prefetched(const EllRow<T, PF> &r, const 
 #ifndef KMSD_STEP_PAIR_F64
 #define KMSD_STEP_PAIR_F64 1  // the paired form for FP64 vectors too
 #endif
+#ifndef KMSD_PAIR_SUM32
+#define KMSD_PAIR_SUM32 0  // 1: the paired complex64 step forms each row's products in FP32
+#endif
 #ifndef KMSD_STEP_PAIR_PREFETCH
 #define KMSD_STEP_PAIR_PREFETCH 0  // rows of the next pair loaded ahead: 0 ELL, 1 + T_{k-2}, 2 + T_{k-1}
 #endif
@@ -599,8 +602,15 @@ __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_S
                     const T ti = rdiv(hv.im[c] - cen * x.im[c], hal, a.inv_half);
                     nx.re[c] = a.first ? tr : T(2) * tr - pv.re[c];
                     nx.im[c] = a.first ? ti : T(2) * ti - pv.im[c];
-                    acc0[0][c].x += (double)x.re[c] * (double)x.re[c] + (double)x.im[c] * (double)x.im[c];
-                    acc1[0][c].x += (double)x.re[c] * (double)nx.re[c] + (double)x.im[c] * (double)nx.im[c];
+                    if (KMSD_PAIR_SUM32 && sizeof(T) == 4) {
+                        // the row's products in the vectors' precision (one
+                        // rounding each), the sums over rows in FP64
+                        acc0[0][c].x += (double)fma(x.re[c], x.re[c], x.im[c] * x.im[c]);
+                        acc1[0][c].x += (double)fma(x.re[c], nx.re[c], x.im[c] * nx.im[c]);
+                    } else {
+                        acc0[0][c].x += (double)x.re[c] * (double)x.re[c] + (double)x.im[c] * (double)x.im[c];
+                        acc1[0][c].x += (double)x.re[c] * (double)nx.re[c] + (double)x.im[c] * (double)nx.im[c];
+                    }
                 }
                 st(a.next + (r2 ? oB : oA), nx);
             }
