@@ -435,8 +435,14 @@ __device__ __forceinline__ void gather_prefetched(const EllRow<T, PF> &r, const 
 #ifndef KMSD_STEP_PAIR_F64
 #define KMSD_STEP_PAIR_F64 1  // the paired form for FP64 vectors too
 #endif
+// The paired complex64 doubling step forms each row's two products
+// (|x|^2 and Re conj(x) next) in FP32 with one FMA and adds them to the FP64
+// column sums, instead of converting the four factors to FP64 first.  On the
+// 4.19M-site honeycomb at R=64 this measured 4.159e11 / 4.152e11 against
+// 4.050e11 / 4.077e11 orbital*moment*vec/s (1690 MHz), and the moments' error
+// against the FP64 path went from 8.9e-8 to 9.8e-8 (norm-wise).
 #ifndef KMSD_PAIR_SUM32
-#define KMSD_PAIR_SUM32 0  // 1: the paired complex64 step forms each row's products in FP32
+#define KMSD_PAIR_SUM32 1
 #endif
 #ifndef KMSD_STEP_PAIR_PREFETCH
 #define KMSD_STEP_PAIR_PREFETCH 0  // rows of the next pair loaded ahead: 0 ELL, 1 + T_{k-2}, 2 + T_{k-1}
@@ -453,6 +459,9 @@ constexpr bool step_pairs() {
 // step against 8.13 / 16.1 ms unbounded and 8.14 / 8.78 ms at 2.
 #ifndef KMSD_SERIES_MINB
 #define KMSD_SERIES_MINB 3
+#endif
+#ifndef KMSD_SERIES_MINB_F64
+#define KMSD_SERIES_MINB_F64 KMSD_SERIES_MINB
 #endif
 // The series step loads a row's Bessel accumulator with its other row-local
 // operands, before the gathers, instead of after the row's arithmetic.
@@ -525,7 +534,8 @@ __device__ __forceinline__ void group_sync(const RowMap &mp, int g) {
 template <class T, int MU, int MODE, int HSRC, bool INLINE_V>
 __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_STEP_PAIR_MINB
                                         : MU == 1 && MODE != MODE_SERIES ? KMSD_STEP_MINB
-                                        : MU == 1 ? KMSD_SERIES_MINB : 1))
+                                        : MU == 1 ? (sizeof(T) == 8 ? KMSD_SERIES_MINB_F64 : KMSD_SERIES_MINB)
+                                                  : 1))
     cheb_step_kernel(const StepArgs<T> a) {
     using V = typename Unit<T>::vec;
     constexpr int C = Unit<T>::C;
