@@ -119,8 +119,7 @@ __global__ void __launch_bounds__(256) batch_step_kernel(const BatchArgs<T> a) {
 #pragma unroll
                     for (int c = 0; c < C; ++c) {
                         const Pk<T> &x = xo[m];
-                        acc0[m][c].x += (double)x.re[c] * x.re[c] + (double)x.im[c] * x.im[c];
-                        acc1[m][c].x += (double)x.re[c] * nx.re[c] + (double)x.im[c] * nx.im[c];
+                        doubling_sums<T>(acc0[m][c].x, acc1[m][c].x, x.re[c], x.im[c], nx.re[c], nx.im[c]);
                     }
                 }
             }

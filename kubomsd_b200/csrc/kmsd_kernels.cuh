@@ -39,6 +39,29 @@ __device__ __forceinline__ void cmac_cplx(Pk<T> &acc, T vr, T vi, const Pk<T> &x
 __device__ __forceinline__ double rdiv(double a, double s, double inv) { return KMSD_F64_RECIP ? a * inv : a / s; }
 __device__ __forceinline__ float rdiv(float a, float, float inv) { return a * inv; }
 
+// The two product-identity sums of one row element: |x|^2 and Re(conj(x) next),
+// added to FP64 column sums.  Every complex64 doubling step (paired, generic,
+// tiled, batched) forms the two products in FP32 with one FMA each
+// (KMSD_PAIR_SUM32), so all entry points compute the same mixed form;
+// complex128 rows form them in FP64.  Against converting the four factors
+// to FP64 first, the paired step on the 4.19M-site honeycomb at R=64 measured
+// 4.159e11 / 4.152e11 against 4.050e11 / 4.077e11 orbital*moment*vec/s
+// (1690 MHz), and the moments' error against the FP64 path went from 8.9e-8
+// to 9.8e-8 (norm-wise).
+#ifndef KMSD_PAIR_SUM32
+#define KMSD_PAIR_SUM32 1
+#endif
+template <class T>
+__device__ __forceinline__ void doubling_sums(double &s0, double &s1, T xr, T xi, T nr, T ni) {
+    if (KMSD_PAIR_SUM32 && sizeof(T) == 4) {
+        s0 += (double)fma(xr, xr, xi * xi);
+        s1 += (double)fma(xr, nr, xi * ni);
+    } else {
+        s0 += (double)xr * (double)xr + (double)xi * (double)xi;
+        s1 += (double)xr * (double)nr + (double)xi * (double)ni;
+    }
+}
+
 // acc[m] += sum_k A[row,k] X[k, unit u_m]   for the MU units of this lane.
 template <class T, int MU>
 __device__ __forceinline__ void gather_row(const CsrView<T> &A, const typename Unit<T>::vec *X,
@@ -435,15 +458,7 @@ __device__ __forceinline__ void gather_prefetched(const EllRow<T, PF> &r, const 
 #ifndef KMSD_STEP_PAIR_F64
 #define KMSD_STEP_PAIR_F64 1  // the paired form for FP64 vectors too
 #endif
-// The paired complex64 doubling step forms each row's two products
-// (|x|^2 and Re conj(x) next) in FP32 with one FMA and adds them to the FP64
-// column sums, instead of converting the four factors to FP64 first.  On the
-// 4.19M-site honeycomb at R=64 this measured 4.159e11 / 4.152e11 against
-// 4.050e11 / 4.077e11 orbital*moment*vec/s (1690 MHz), and the moments' error
-// against the FP64 path went from 8.9e-8 to 9.8e-8 (norm-wise).
-#ifndef KMSD_PAIR_SUM32
-#define KMSD_PAIR_SUM32 1
-#endif
+
 #ifndef KMSD_STEP_PAIR_PREFETCH
 #define KMSD_STEP_PAIR_PREFETCH 0  // rows of the next pair loaded ahead: 0 ELL, 1 + T_{k-2}, 2 + T_{k-1}
 #endif
@@ -612,15 +627,7 @@ __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_S
                     const T ti = rdiv(hv.im[c] - cen * x.im[c], hal, a.inv_half);
                     nx.re[c] = a.first ? tr : T(2) * tr - pv.re[c];
                     nx.im[c] = a.first ? ti : T(2) * ti - pv.im[c];
-                    if (KMSD_PAIR_SUM32 && sizeof(T) == 4) {
-                        // the row's products in the vectors' precision (one
-                        // rounding each), the sums over rows in FP64
-                        acc0[0][c].x += (double)fma(x.re[c], x.re[c], x.im[c] * x.im[c]);
-                        acc1[0][c].x += (double)fma(x.re[c], nx.re[c], x.im[c] * nx.im[c]);
-                    } else {
-                        acc0[0][c].x += (double)x.re[c] * (double)x.re[c] + (double)x.im[c] * (double)x.im[c];
-                        acc1[0][c].x += (double)x.re[c] * (double)nx.re[c] + (double)x.im[c] * (double)nx.im[c];
-                    }
+                    doubling_sums<T>(acc0[0][c].x, acc1[0][c].x, x.re[c], x.im[c], nx.re[c], nx.im[c]);
                 }
                 st(a.next + (r2 ? oB : oA), nx);
             }
@@ -755,8 +762,7 @@ __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_S
             if (MODE == MODE_DOUBLING) {
 #pragma unroll
                 for (int c = 0; c < C; ++c) {
-                    acc0[m][c].x += (double)x.re[c] * (double)x.re[c] + (double)x.im[c] * (double)x.im[c];
-                    acc1[m][c].x += (double)x.re[c] * (double)nx.re[c] + (double)x.im[c] * (double)nx.im[c];
+                    doubling_sums<T>(acc0[m][c].x, acc1[m][c].x, x.re[c], x.im[c], nx.re[c], nx.im[c]);
                 }
             }
             if (MODE == MODE_SERIES) {

@@ -319,11 +319,8 @@ __global__ void __launch_bounds__(kTileThreads, KMSD_TILE_MINB)
                                                 (double)br.im[c] * (double)nx.im[c];
                         } else {
 #pragma unroll
-                            for (int c = 0; c < C; ++c) {
-                                acc0[0][c].x += (double)x.re[c] * (double)x.re[c] + (double)x.im[c] * (double)x.im[c];
-                                acc1[0][c].x +=
-                                    (double)x.re[c] * (double)nx.re[c] + (double)x.im[c] * (double)nx.im[c];
-                            }
+                            for (int c = 0; c < C; ++c)
+                                doubling_sums<T>(acc0[0][c].x, acc1[0][c].x, x.re[c], x.im[c], nx.re[c], nx.im[c]);
                         }
                     }
                 }
