@@ -49,6 +49,7 @@ template <class T> struct BatchArgs {
     const V *bra;
     const V *hx;  // HSRC_SOLVED: the operator already applied (S^-1 H T_k)
     int first;
+    int exact_sums;    // MODE_DOUBLING: FP64 row products (mu_0, mu_1 of a direct-moments call)
     double2 *partial;  // [ntiles][ncol] (x2 for doubling)
 };
 
@@ -119,7 +120,7 @@ __global__ void __launch_bounds__(256) batch_step_kernel(const BatchArgs<T> a) {
 #pragma unroll
                     for (int c = 0; c < C; ++c) {
                         const Pk<T> &x = xo[m];
-                        doubling_sums<T>(acc0[m][c].x, acc1[m][c].x, x.re[c], x.im[c], nx.re[c], nx.im[c]);
+                        doubling_sums<T>(acc0[m][c].x, acc1[m][c].x, x.re[c], x.im[c], nx.re[c], nx.im[c], a.exact_sums);
                     }
                 }
             }
@@ -323,6 +324,7 @@ int record(kmsd_batch_s *bt, const double2 *B, double *mu, int64_t b, int64_t le
         a.first = k == 1;
         int rc;
         if (k == 1 || doubling) {
+            a.exact_sums = !doubling;
             rc = launch_batch_step<T, MU, MODE_DOUBLING>(bt, a, s);
             batch_finalize_kernel<MODE_DOUBLING><<<(int)bt->ninst, 128, 0, s>>>(
                 a.partial, bt->tiles.seg_tile0, ncol, (int)b, mu, length, k - 1);

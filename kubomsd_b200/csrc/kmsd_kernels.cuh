@@ -51,9 +51,12 @@ __device__ __forceinline__ float rdiv(float a, float, float inv) { return a * in
 #ifndef KMSD_PAIR_SUM32
 #define KMSD_PAIR_SUM32 1
 #endif
+// `exact` forms the products in FP64 in every precision: the first launch of
+// a direct-moments call that takes mu_0 and mu_1 from these sums (the batch and
+// the allocation-free entry point) matches the direct path's FP64 products.
 template <class T>
-__device__ __forceinline__ void doubling_sums(double &s0, double &s1, T xr, T xi, T nr, T ni) {
-    if (KMSD_PAIR_SUM32 && sizeof(T) == 4) {
+__device__ __forceinline__ void doubling_sums(double &s0, double &s1, T xr, T xi, T nr, T ni, bool exact = false) {
+    if (KMSD_PAIR_SUM32 && sizeof(T) == 4 && !exact) {
         s0 += (double)fma(xr, xr, xi * xi);
         s1 += (double)fma(xr, nr, xi * ni);
     } else {
@@ -358,6 +361,7 @@ template <class T> struct StepArgs {
     const V *prev;         // T_{k-2}; may alias `next`
     V *next;               // T_k
     int first;             // k == 1
+    int exact_sums;        // MODE_DOUBLING: FP64 row products in every precision
     double center, half;
     T inv_half;
     // moments
@@ -627,7 +631,7 @@ __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_S
                     const T ti = rdiv(hv.im[c] - cen * x.im[c], hal, a.inv_half);
                     nx.re[c] = a.first ? tr : T(2) * tr - pv.re[c];
                     nx.im[c] = a.first ? ti : T(2) * ti - pv.im[c];
-                    doubling_sums<T>(acc0[0][c].x, acc1[0][c].x, x.re[c], x.im[c], nx.re[c], nx.im[c]);
+                    doubling_sums<T>(acc0[0][c].x, acc1[0][c].x, x.re[c], x.im[c], nx.re[c], nx.im[c], a.exact_sums);
                 }
                 st(a.next + (r2 ? oB : oA), nx);
             }
@@ -762,7 +766,7 @@ __global__ void __launch_bounds__(256, (step_pairs<T, MU, MODE, HSRC>() ? KMSD_S
             if (MODE == MODE_DOUBLING) {
 #pragma unroll
                 for (int c = 0; c < C; ++c) {
-                    doubling_sums<T>(acc0[m][c].x, acc1[m][c].x, x.re[c], x.im[c], nx.re[c], nx.im[c]);
+                    doubling_sums<T>(acc0[m][c].x, acc1[m][c].x, x.re[c], x.im[c], nx.re[c], nx.im[c], a.exact_sums);
                 }
             }
             if (MODE == MODE_SERIES) {

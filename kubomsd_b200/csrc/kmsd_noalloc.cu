@@ -202,6 +202,7 @@ int run(kmsd_engine_s *e, const double2 *B, double *mu, int64_t b, int64_t lengt
         a.first = k == 1;
         if (k == 1 || doubling) {
             a.kmom = k - 1;
+            a.exact_sums = !doubling;
             cheb_step_kernel<T, MU, MODE_DOUBLING, HSRC_CSR, false><<<g_first, kThreads, smem, s>>>(a);
         } else {
             a.kmom = k;

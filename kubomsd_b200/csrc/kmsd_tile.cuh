@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(kTileThreads, KMSD_TILE_MINB)
                         } else {
 #pragma unroll
                             for (int c = 0; c < C; ++c)
-                                doubling_sums<T>(acc0[0][c].x, acc1[0][c].x, x.re[c], x.im[c], nx.re[c], nx.im[c]);
+                                doubling_sums<T>(acc0[0][c].x, acc1[0][c].x, x.re[c], x.im[c], nx.re[c], nx.im[c], a.exact_sums);
                         }
                     }
                 }
