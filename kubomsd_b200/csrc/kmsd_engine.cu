@@ -129,35 +129,41 @@ int Reducer::ensure(int grid, int ncol, int copies) {
 }  // namespace kmsd
 
 // ------------------------------------------------------------------ CSR
+// The complex64 copies of an uploaded matrix, built on first use.  Engine
+// replicas on several host threads share one matrix, so the build runs under
+// one lock and the pointers are published only once their values are on the
+// device: a second caller never sees an allocated but unfilled copy.
 int kmsd_csr_s::ensure_f32() {
+    static std::mutex lock;
+    std::lock_guard<std::mutex> guard(lock);
     if (re32) return KMSD_OK;
-    std::vector<double> h(nnz);
-    std::vector<float> f(nnz);
-    KMSD_CUDA(cudaMemcpy(h.data(), re64, nnz * sizeof(double), cudaMemcpyDeviceToHost));
-    for (int64_t i = 0; i < nnz; ++i) f[i] = (float)h[i];
-    KMSD_CUDA(cudaMalloc(&re32, std::max<int64_t>(nnz, 1) * sizeof(float)));
-    KMSD_CUDA(cudaMemcpy(re32, f.data(), nnz * sizeof(float), cudaMemcpyHostToDevice));
-    if (complex_values) {
-        KMSD_CUDA(cudaMemcpy(h.data(), im64, nnz * sizeof(double), cudaMemcpyDeviceToHost));
-        for (int64_t i = 0; i < nnz; ++i) f[i] = (float)h[i];
-        KMSD_CUDA(cudaMalloc(&im32, std::max<int64_t>(nnz, 1) * sizeof(float)));
-        KMSD_CUDA(cudaMemcpy(im32, f.data(), nnz * sizeof(float), cudaMemcpyHostToDevice));
+    float *dre = nullptr, *dim = nullptr, *dere = nullptr, *deim = nullptr;
+    auto fail_free = [&](cudaError_t err) {
+        for (float *q : {dre, dim, dere, deim})
+            if (q) cudaFree(q);
+        return fail(KMSD_ECUDA, cudaGetErrorString(err));
+    };
+    // d = (float) src for `count` values of a device FP64 array
+    auto convert = [&](const double *src, int64_t count, float **d) -> cudaError_t {
+        std::vector<double> h(std::max<int64_t>(count, 1));
+        std::vector<float> f(h.size());
+        cudaError_t err = cudaMemcpy(h.data(), src, count * sizeof(double), cudaMemcpyDeviceToHost);
+        if (err != cudaSuccess) return err;
+        for (int64_t i = 0; i < count; ++i) f[i] = (float)h[i];
+        if ((err = cudaMalloc(d, f.size() * sizeof(float))) != cudaSuccess) return err;
+        return cudaMemcpy(*d, f.data(), count * sizeof(float), cudaMemcpyHostToDevice);
+    };
+    cudaError_t err = convert(re64, nnz, &dre);
+    if (err == cudaSuccess && complex_values) err = convert(im64, nnz, &dim);
+    if (err == cudaSuccess && ell_w > 0) {
+        err = convert(ell_re64, n * ell_w, &dere);
+        if (err == cudaSuccess && complex_values) err = convert(ell_im64, n * ell_w, &deim);
     }
-    if (ell_w > 0) {
-        const int64_t m = n * ell_w;
-        std::vector<double> he(m);
-        std::vector<float> fe(m);
-        KMSD_CUDA(cudaMemcpy(he.data(), ell_re64, m * sizeof(double), cudaMemcpyDeviceToHost));
-        for (int64_t i = 0; i < m; ++i) fe[i] = (float)he[i];
-        KMSD_CUDA(cudaMalloc(&ell_re32, m * sizeof(float)));
-        KMSD_CUDA(cudaMemcpy(ell_re32, fe.data(), m * sizeof(float), cudaMemcpyHostToDevice));
-        if (complex_values) {
-            KMSD_CUDA(cudaMemcpy(he.data(), ell_im64, m * sizeof(double), cudaMemcpyDeviceToHost));
-            for (int64_t i = 0; i < m; ++i) fe[i] = (float)he[i];
-            KMSD_CUDA(cudaMalloc(&ell_im32, m * sizeof(float)));
-            KMSD_CUDA(cudaMemcpy(ell_im32, fe.data(), m * sizeof(float), cudaMemcpyHostToDevice));
-        }
-    }
+    if (err != cudaSuccess) return fail_free(err);
+    im32 = dim;
+    ell_re32 = dere;
+    ell_im32 = deim;
+    re32 = dre;  // last: the copy counts as built once re32 is set
     return KMSD_OK;
 }
 

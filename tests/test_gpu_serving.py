@@ -57,3 +57,52 @@ def test_admission_waits_for_hbm_budget(models):
     assert len(res) == 3
     spans = sorted((r.start, r.end) for r in res)
     assert all(spans[i + 1][0] >= spans[i][1] - 1e-3 for i in range(2))  # admitted one after another
+
+
+@pytest.mark.parametrize("kind", ["moments", "series"])
+def test_replicas_first_use_concurrently(cuda, kind):
+    """Engine replicas share one uploaded model and build its complex64 copy on
+    first use.  Replicas whose first mixed-precision calls start at the same
+    time on two host threads and streams return exactly what one call alone
+    returns (the copy is published only once it is complete)."""
+    import threading
+    from kubomsd_b200 import kpm, lattices
+    from kubomsd_b200.config import RunConfig
+    from kubomsd_b200.operators import build_operators
+    torch = cuda
+    m = lattices.honeycomb(256, 128, seed=9)
+    cfg = RunConfig(energy_eV=[0.], time_fs=[0., 1.], spectral_bounds=(-9.2, 9.2), axes=("x",), include_vac=False,
+                    precision="mixed", moment_doubling=True)
+    c, a = kpm.scaling(cfg)
+    B = torch.from_numpy(kpm.random_phases(m.n, 4, range(8))).cuda()
+    coeff, _ = kpm.bessel_coefficients(.5, cfg, weighted_tail=True)
+    aug = torch.cat([B, torch.zeros_like(B)], dim=1).contiguous()
+
+    def call(eng):
+        if kind == "moments":
+            return eng.moments(B, 64, c, a).cpu().numpy()
+        return eng.series(aug, coeff, c, a, [[1., 0., 0.]]).cpu().numpy()
+
+    engines = [build_operators(m, cfg).native]
+    engines.append(engines[0].replica())
+    out, errors = [None, None], []
+    gate = threading.Barrier(2)
+
+    def worker(i):
+        try:
+            with torch.cuda.stream(torch.cuda.Stream()):
+                gate.wait(timeout=30)
+                out[i] = call(engines[i])
+        except Exception as exc:  # noqa: BLE001
+            errors.append(exc)
+
+    threads = [threading.Thread(target=worker, args=(i,)) for i in range(2)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join(timeout=120)
+    assert not errors, errors
+    alone = call(engines[0])
+    for got in out:
+        assert np.isfinite(got).all()
+        np.testing.assert_array_equal(got, alone)
