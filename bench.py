@@ -292,8 +292,8 @@ def _bench_call(fn, sync):
 def config_c1(threads):
     """Config 1 in full: 64 x 64 square lattice, R=8, M=512, 201 energies,
     stepwise MSD along x over 0-50 fs at dt = 1 fs, no VAC; FP64 and mixed,
-    moment doubling.  Work in the survey's unit: N per application of the
-    scaled operator to one vector (moment and propagation steps)."""
+    moment doubling.  Work counted as N per application of the scaled
+    operator to one vector (moment and propagation steps)."""
     import torch
     import scipy.sparse as sp
     from kubomsd_b200 import kpm, lattices, stochastic

@@ -47,7 +47,7 @@ namespace kmsd {
 // Vector loads of a row's ELL entries from the stage and 32-bit in-tile
 // offsets: on the 4.19M-site honeycomb at R=64 this took FP64 direct moments
 // from 7.92e10 to 8.91e10, FP64 doubling from 1.60e11 to 1.95e11 and mixed
-// direct from 1.78e11 to 1.93e11 orbital*moment*vec/s (same box, 1800 MHz).
+// direct from 1.78e11 to 1.93e11 orbital*moment*vec/s (one GPU, 1800 MHz).
 #ifndef KMSD_TILE_VEC
 #define KMSD_TILE_VEC 1
 #endif
