@@ -71,8 +71,9 @@ def parse():
     p.add_argument("--no-compare", action="store_true", help="skip the FP64 / direct comparison lines")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-configs", action="store_true",
-                   help="skip the per-configuration blocks (config 1 in full, config 2 at full size, a config-5 "
-                        "serving window)")
+                   help="skip the per-configuration blocks (config 1 in full, config 2 at full size, the "
+                        "config-3 stepwise MSD with the series step, a config-4 batch sample, a config-5 serving "
+                        "window)")
     return p.parse_args()
 
 
