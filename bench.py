@@ -764,9 +764,11 @@ def run_batch(args):
 
 
 def run_serving(args):
-    """Config 5 (shortened): Poisson stream of KPM DOS jobs over resident
+    """Config 5 (shortened): Poisson stream of KPM DOS jobs and stepwise MSD
+    jobs (a fraction KMSD_SERVING_MSD, 0.25 by default) over resident
     orthogonal 2D lattices and nonorthogonal sp3 cells, admitted by an HBM
-    budget of 150 GB into 8 concurrent slots; p50/p99 latency and throughput."""
+    budget of 150 GB into 8 concurrent slots; p50/p99 latency and the DOS
+    jobs' moment throughput."""
     from kubomsd_b200 import lattices
     from kubomsd_b200.serving import ResidentModel, Server, latency_summary, poisson_stream
     models = {
@@ -781,7 +783,8 @@ def run_serving(args):
     }
     duration = float(os.environ.get("KMSD_SERVING_SECONDS", "30"))
     rate = float(os.environ.get("KMSD_SERVING_RATE", "20"))
-    reqs = poisson_stream(rate, duration, models, seed=5)
+    msd = float(os.environ.get("KMSD_SERVING_MSD", "0.25"))  # fraction of stepwise MSD jobs (x axis, 0/1/2 fs)
+    reqs = poisson_stream(rate, duration, models, seed=5, msd_fraction=msd, times_fs=(0., 1., 2.))
     srv = Server(models, slots=8, hbm_budget_bytes=150 * 10 ** 9)
     t0 = time.perf_counter()
     res = srv.serve(reqs)
@@ -793,8 +796,8 @@ def run_serving(args):
                       "warmup": 0, "ms_per_step": wall / max(len(res), 1) * 1e3, "higher_is_better": True,
                       "scaling": "weak", "vs_baseline": None, "dtype": "c64 vectors / f64 accumulation (lattices), "
                       "c128 (sp3)", "data": "synthetic Poisson stream (seed 5)",
-                      "config": {"workload": f"serving: Poisson {rate:g} req/s for {duration:g} s, M in "
-                                             "{512,1024,2048}, R in {8,32}, models "
+                      "config": {"workload": f"serving: Poisson {rate:g} req/s for {duration:g} s, {msd:.0%} "
+                                             "stepwise MSD jobs, M in {512,1024,2048}, R in {8,32}, models "
                                              + ", ".join(f"{k} ({m.n:,} orbitals)" for k, m in models.items())
                                              + ", 8 slots, HBM budget 150 GB"},
                       "latency": summ, "errors": len(srv.errors), "offered_requests": len(reqs),
