@@ -71,13 +71,13 @@ CountOff::~CountOff() { --g_count_off; }
 int64_t CountOff::recorded() const { return g_recorded - start; }
 int64_t launches() { return g_launches.load(std::memory_order_relaxed); }
 int sm_count() {
-    static int cached = 0;
-    if (!cached) {
-        int dev = 0;
+    // initialised once, thread-safely, on the first call
+    static const int cached = [] {
+        int dev = 0, count = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, dev);
-        if (cached <= 0) cached = 148;
-    }
+        cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+        return count > 0 ? count : 148;
+    }();
     return cached;
 }
 int grid_for(int64_t rows, const RowMap &mp) {

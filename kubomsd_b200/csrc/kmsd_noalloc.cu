@@ -61,15 +61,16 @@ std::map<void *, void *> g_scratch_address;  // CUDA context -> device address o
 // no link-time dependency on libcuda).
 int current_context(void **ctx) {
     using GetCurrent = int (*)(void **);
-    static GetCurrent fn = nullptr;
-    if (fn == nullptr) {
+    // looked up once, thread-safely, on the first call
+    static const GetCurrent fn = []() -> GetCurrent {
         void *p = nullptr;
         cudaDriverEntryPointQueryResult q;
-        KMSD_CUDA(cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q));
-        if (q != cudaDriverEntryPointSuccess || p == nullptr)
-            return fail(KMSD_ECUDA, "cuCtxGetCurrent is not available from the driver");
-        fn = reinterpret_cast<GetCurrent>(p);
-    }
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        return reinterpret_cast<GetCurrent>(p);
+    }();
+    if (fn == nullptr) return fail(KMSD_ECUDA, "cuCtxGetCurrent is not available from the driver");
     *ctx = nullptr;
     if (fn(ctx) != 0) return fail(KMSD_ECUDA, "cuCtxGetCurrent failed");
     return KMSD_OK;

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -181,7 +182,11 @@ int launch_step_h(E *e, StepArgs<T> &a, cudaStream_t s) {
 template <class T, int MODE, int W>
 int launch_tile(E *e, StepArgs<T> &a, cudaStream_t s) {
     const auto kern = cheb_tile_kernel<T, MODE, W>;
-    static int smem_cap = 0;  // per instantiation
+    // per instantiation, shared by every calling thread
+    static std::mutex lock;
+    static int smem_cap = 0;
+    static std::map<size_t, int> per_sm_cache;  // shared bytes -> CTAs per SM
+    std::unique_lock<std::mutex> guard(lock);
     if (!smem_cap) {
         int dev = 0, optin = 0;
         KMSD_CUDA(cudaGetDevice(&dev));
@@ -198,7 +203,6 @@ int launch_tile(E *e, StepArgs<T> &a, cudaStream_t s) {
     const TileLayout L = tile_layout(tr, mp.U, W, nvec, (int)sizeof(T));
     const size_t sm = tile_smem(L, mp, Unit<T>::C);
     if (sm > (size_t)smem_cap) return fail(KMSD_EINVAL, "tile step does not fit in shared memory");
-    static std::map<size_t, int> per_sm_cache;  // per instantiation: shared bytes -> CTAs per SM
     int per_sm = 0;
     auto it = per_sm_cache.find(sm);
     if (it != per_sm_cache.end()) {
@@ -208,6 +212,7 @@ int launch_tile(E *e, StepArgs<T> &a, cudaStream_t s) {
         per_sm = std::max(per_sm, 1);
         per_sm_cache[sm] = per_sm;
     }
+    guard.unlock();
     const int64_t ntiles = (a.n + tr - 1) / tr;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)sm_count() * per_sm));
     if (e->red.ensure(grid, mp.U * Unit<T>::C, 2)) return KMSD_ECUDA;
