@@ -206,6 +206,24 @@ def pcg_known():
     return out
 
 
+TIME_GRIDS = [(50., 1.), (1., .1), (.3, .1), (10., .7), (5., .5), (0., 1.), (2., 3.), (100., .01), (7.3, .25)]
+ENERGY_GRIDS = [(-11., 11., 201), (-9., 9., 201), (-1., 1., 2), (-40., 40., 13), (.1, .7, 7)]
+
+
+def config_case():
+    """The reference's output grids (config.py:14-24): time grids from (tmax,
+    dt) and energy grids from (emin, emax, n), which must match bit for bit."""
+    from kubo_msd.config import resolve_output_grid, resolve_time_grid
+    out = {}
+    for i, (tmax, dt) in enumerate(TIME_GRIDS):
+        out[f"time_{i}"] = np.asarray(resolve_time_grid(tmax, dt))
+    for i, (a, b, n) in enumerate(ENERGY_GRIDS):
+        out[f"energy_{i}"] = np.asarray(resolve_output_grid(a, b, n))
+    out["time_inputs"] = np.asarray(TIME_GRIDS)
+    out["energy_inputs"] = np.asarray(ENERGY_GRIDS)
+    return out
+
+
 def statistics_case():
     """The reference's paired block bootstrap (observables/statistics.py:5-22)
     on seeded block sums: 9 blocks of unequal counts over (axis, time,
@@ -381,6 +399,7 @@ CASES = {
     "pcg_known": pcg_known,
     "host_formulas": host_formulas,
     "statistics": statistics_case,
+    "config": config_case,
     "square16_pipeline": square_pipeline,
     "square16_pipeline_vac": lambda: square_pipeline("stepwise", include_vac=True),
     "square16_pipeline_spectral": lambda: square_pipeline("spectral", include_vac=False),

@@ -184,3 +184,31 @@ def test_series_row_bytes():
     # complex64 [psi | phi] of 2 x 64 columns on a 4-wide ELL operator
     assert bench.series_row_bytes(128, 4, 4) == 5 * 128 * 8 + 4 * 8 + 2 * 4 * 4
     assert bench.series_row_bytes(64, 8, 4) == 5 * 64 * 16 + 4 * 12 + 2 * 4 * 8
+
+
+# ------------------------------------------------------------ output grids
+def test_output_grids_match_reference_bit_for_bit():
+    """Time and energy grids from the reference's resolve_time_grid /
+    resolve_output_grid (tests/golden/config.npz): identical bits, since every
+    moment, propagation and MSD array is indexed by them."""
+    from kubomsd_b200.config import resolve_output_grid, resolve_time_grid
+    d = golden("config")
+    for i, (tmax, dt) in enumerate(d["time_inputs"]):
+        np.testing.assert_array_equal(resolve_time_grid(float(tmax), float(dt)), d[f"time_{i}"])
+    for i, (a, b, n) in enumerate(d["energy_inputs"]):
+        np.testing.assert_array_equal(resolve_output_grid(float(a), float(b), int(n)), d[f"energy_{i}"])
+
+
+@pytest.mark.parametrize("call,message", [
+    (lambda c: c.resolve_time_grid(-1., 1.), "invalid tmax/dt"),
+    (lambda c: c.resolve_time_grid(1., 0.), "invalid tmax/dt"),
+    (lambda c: c.resolve_time_grid(np.inf, 1.), "invalid tmax/dt"),
+    (lambda c: c.resolve_output_grid(1., 1., 5), "require finite emin < emax"),
+    (lambda c: c.resolve_output_grid(0., 1., 1), "require finite emin < emax"),
+    (lambda c: c.grid([0., 1., 1.], "energy"), "energy must be a finite, strictly increasing"),
+    (lambda c: c.grid([.5, 1.], "time", True), "time must start at zero"),
+])
+def test_grid_errors_match_reference_messages(call, message):
+    from kubomsd_b200 import config
+    with pytest.raises(Exception, match=message):
+        call(config)
